@@ -1,0 +1,157 @@
+/*
+ * nsx.h -- C ABI of the B200 (sm_100a) Lanczos hot path for pn-factorised
+ * J-scheme shell-model Hamiltonians (the NuLnz / NuTRL solver of NuShellX).
+ *
+ * The reference has no library API: its hot path is a set of Fortran module
+ * subroutines working on module globals.  Each entry point below replaces one
+ * of them (cited file:line relative to the NuShellX source tree):
+ *
+ *   nsx_create / nsx_load_files  <- Lnz_TRD setup          src/NuLnz/NuCoreX.f90:807-1367
+ *                                   (+ drdbh pn table        src/NuLnz/NuCoreX.f90:1428-1577)
+ *   nsx_matvec                   <- multiplyx(); multiplya(); multiplyb()
+ *                                                           src/NuLnz/NuCoreX.f90:76-226
+ *   nsx_solve                    <- Lnz_OP + lnzort (standard and thick restart)
+ *                                                           src/NuLnz/NuCoreX.f90:240-791
+ *   nsx_destroy                  <- (module deallocation at program end)
+ *
+ * Conventions: every function returns 0 on success or a negative NSX_E* code;
+ * nsx_last_error() gives the message of the last failure on the calling
+ * thread.  No exceptions or aborts cross this boundary.  A handle is used by
+ * one host thread at a time; all device work goes to the stream passed in
+ * (NULL = the legacy default stream).  Vectors are FP64 in the reference's
+ * layout: blocks (2Ja,2Jb) in ascending order, each a column-major
+ * d_a(Ja) x d_b(Jb) matrix with proton partitions along the rows.
+ */
+#ifndef NSX_H
+#define NSX_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NSX_OK 0
+#define NSX_E_ARG (-1)      /* invalid argument / inconsistent problem data */
+#define NSX_E_IO (-2)       /* file missing, short or malformed record      */
+#define NSX_E_CUDA (-3)     /* CUDA runtime failure                          */
+#define NSX_E_NOMEM (-4)    /* device or host allocation failed              */
+#define NSX_E_NUMERIC (-5)  /* NaN/Inf in the recurrence, eigensolver failure */
+#define NSX_E_NOCONV (-6)   /* iteration limit reached before convergence    */
+
+#define NSX_FP64 0          /* matvec contractions in FP64                   */
+#define NSX_FP32 1          /* matvec contractions in FP32, FP64 in/out      */
+
+/* One nucleon species, in the content and order of its .tri/.trd/.mat files
+ * (src/NuOpd/NuOpd.f90:484-494, 678-680; src/NuOrth/NuOrth.f90:218-223). */
+typedef struct nsx_species {
+  int32_t nspart;            /* number of partitions                            */
+  int32_t minJ2, maxJ2;      /* 2J range of the species (step 2)                */
+  const int32_t *njt;        /* [nJ][nspart]: nJT(partition, J), nJ=(maxJ2-minJ2)/2+1 */
+  const int32_t *parity;     /* [nspart]: +1 / -1                               */
+  int32_t shell_first;       /* global number (1-based) of the species' first shell */
+  int32_t nshell;            /* number of shells of the species                 */
+  /* one-body reduced densities, one entry per .trd key */
+  int32_t nkeys;
+  const uint8_t *keys;       /* [nkeys][8]: 2Jl, 2Jr, shell_l, shell_r, 2lam, 0,0,0 */
+  const int64_t *val_off;    /* [nkeys+1]: offsets into vals                    */
+  const double *vals;        /* values in .trd order (per right partition r, left l
+                                with bit l of mask r: nJT(l,Jl) x nJT(r,Jr) col-major) */
+  int32_t words;             /* 32-bit mask words per partition                 */
+  const uint32_t *masks;     /* [nkeys][nspart][words]                          */
+  /* like-particle Hamiltonian segments (.mat), npr >= np */
+  int32_t nseg;
+  const int32_t *seg_J2;     /* [nseg]                                          */
+  const int32_t *seg_np;     /* [nseg] left partition (1-based, as in .mat)     */
+  const int32_t *seg_npr;    /* [nseg] right partition (1-based), >= seg_np      */
+  const int64_t *seg_off;    /* [nseg+1] offsets into seg_vals                  */
+  const double *seg_vals;    /* matrix(dimptr, dimpt) column-major per segment  */
+} nsx_species;
+
+typedef struct nsx_problem {
+  int32_t J2;                /* total 2J                                        */
+  int32_t parity;            /* +1, -1, or 0 for both (the reference's Tparity) */
+  nsx_species a;             /* species "a" (protons)                           */
+  nsx_species b;             /* species "b" (neutrons)                          */
+  int32_t nop;               /* pn multipole matrix elements (.oph)             */
+  const uint8_t *op_keys;    /* [nop][8]: shell_al, shell_ar, shell_bl, shell_br, 2lam, 0,0,0 */
+  const double *op_vals;     /* [nop] V_lam in MeV (before renorm)              */
+  double renorm;             /* .spe line 2 (src/NuLnz/NuCoreX.f90:1664-1670)   */
+} nsx_problem;
+
+typedef struct nsx_params {
+  int32_t nev;               /* eigenpairs wanted (reference: no_level)         */
+  int32_t max_iter;          /* total Lanczos steps allowed                     */
+  int32_t window;            /* thick-restart window (basis vectors kept in HBM)*/
+  int32_t keep;              /* Ritz vectors kept at a restart (0 = automatic)  */
+  double tol;                /* residual tolerance ||H y - theta y|| (MeV)      */
+  int32_t precision;         /* NSX_FP64 or NSX_FP32                            */
+  int32_t pre_iter;          /* power pre-iterations on the start vector (ref: 2) */
+  uint64_t seed;             /* start-vector seed                               */
+  const double *start;       /* optional host start vector [no_state] or NULL   */
+  int32_t refine;            /* 1: FP64 Rayleigh-Ritz refinement of the result  */
+} nsx_params;
+
+typedef struct nsx_report {
+  int32_t iterations;        /* Lanczos steps (matvecs after the pre-iterations) */
+  int32_t matvecs;           /* all H.v products, including pre-iterations       */
+  int32_t restarts;
+  int32_t converged;         /* number of eigenpairs with residual <= tol       */
+  double seconds;            /* wall time of nsx_solve                          */
+  double matvec_seconds;     /* device time in H.v                              */
+  double residual[64];       /* residual norms of the first min(nev,64) pairs    */
+} nsx_report;
+
+typedef struct nsx_handle nsx_handle;
+
+/* Build a solver handle from host arrays.  The library copies what it needs
+ * to the device; the caller keeps ownership of the host buffers. */
+int nsx_create(const nsx_problem *prob, int device, nsx_handle **out);
+
+/* The reference's input file set (src/NuLnz/NuCoreX.f90:1659-1670, 1216-1319).
+ * Files read: <a>.tri <a>.trd <b>.tri <b>.trd <inter>.oph <inter>.spe and, for every
+ * 2J of each species, <like>file_code(J, T2/2, nmp/2+36)<xtra>.sgt / .mat
+ * (src/NuCommon/NuModules.F90:553-597). */
+typedef struct nsx_files {
+  const char *a, *b, *inter;      /* base names (paths without extension)        */
+  const char *like_a, *like_b;    /* nucleus prefix of the .sgt/.mat files        */
+  int32_t T2_a, nmp_a;            /* file-code arguments of species a            */
+  int32_t T2_b, nmp_b;            /* file-code arguments of species b            */
+  char xtra;                      /* character between file code and extension   */
+  int32_t J2, parity;             /* target 2J and parity (0 = both)             */
+  int32_t nshells;                /* shells of the model space (protons first)   */
+  int32_t nshells_p;              /* how many of them are proton shells          */
+  const int32_t *shell_parity;    /* [nshells] +1/-1 (the .nus file's sp(i))      */
+} nsx_files;
+
+int nsx_load_files(const nsx_files *files, int device, nsx_handle **out);
+
+/* The 3-character NuShellX file code (src/NuCommon/NuModules.F90:22-35). */
+int nsx_file_code(int32_t i, int32_t j, int32_t k, char out[4]);
+
+int64_t nsx_dim(const nsx_handle *h);          /* no_state (both parities)   */
+int32_t nsx_nblocks(const nsx_handle *h);
+/* Block list: [nblocks][4] = 2Ja, 2Jb, d_a, d_b, and offsets [nblocks+1]. */
+int nsx_blocks(const nsx_handle *h, int32_t *blocks4, int64_t *offsets);
+/* Parity mask (the reference's lcoef): [no_state] bytes 0/1. */
+int nsx_lcoef(const nsx_handle *h, uint8_t *mask);
+/* Algorithmic flop count of one H.v (partition-sparse, reuse-aware). */
+double nsx_matvec_flops(const nsx_handle *h);
+
+/* y = H x.  x and y are DEVICE pointers of no_state doubles (stream-ordered). */
+int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, void *stream);
+/* The same with HOST pointers: copies in, multiplies, copies out, synchronises. */
+int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision);
+
+/* Lowest nev eigenpairs.  evals: host [nev]; evecs: host [nev][no_state] or NULL. */
+int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs,
+              nsx_report *report);
+
+void nsx_destroy(nsx_handle *h);
+const char *nsx_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,152 @@
+// extern "C" entry points of libnsx (declared in include/nsx.h).  Every call
+// catches internal failures and turns them into a negative return code plus a
+// thread-local message: nothing is thrown or aborted across the boundary.
+#include <cstring>
+#include <memory>
+#include <exception>
+#include <new>
+#include "nsx_internal.h"
+
+namespace nsx {
+static thread_local std::string g_err;
+void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+void check_cuda(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  int code = (e == cudaErrorMemoryAllocation) ? NSX_E_NOMEM : NSX_E_CUDA;
+  throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+void solve(nsx_handle *h, const nsx_params *P, double *evals, double *evecs, nsx_report *rep);
+std::shared_ptr<void> load_files(const nsx_files *f, nsx_problem *p);
+
+template <typename F>
+static int guarded(F &&f) {
+  try {
+    f();
+    return NSX_OK;
+  } catch (const Error &e) {
+    g_err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_err = "host allocation failed";
+    return NSX_E_NOMEM;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return NSX_E_ARG;
+  } catch (...) {
+    g_err = "unknown failure";
+    return NSX_E_ARG;
+  }
+}
+}  // namespace nsx
+
+using namespace nsx;
+
+extern "C" {
+
+const char *nsx_last_error(void) { return g_err.c_str(); }
+
+int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
+  if (!out) {
+    g_err = "null output handle pointer";
+    return NSX_E_ARG;
+  }
+  *out = nullptr;
+  nsx_handle *h = new (std::nothrow) nsx_handle();
+  if (!h) {
+    g_err = "host allocation failed";
+    return NSX_E_NOMEM;
+  }
+  int rc = guarded([&] {
+    if (!prob) fail(NSX_E_ARG, "null problem");
+    h->device = device;
+    NSX_CUDA(cudaSetDevice(device));
+    build_plan(h, prob);
+    upload(h);
+  });
+  if (rc != NSX_OK) {
+    release(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return NSX_OK;
+}
+
+int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
+  nsx_problem p;
+  std::memset(&p, 0, sizeof(p));
+  std::shared_ptr<void> store;
+  int rc = guarded([&] {
+    if (!files || !out) fail(NSX_E_ARG, "null argument");
+    store = load_files(files, &p);
+  });
+  if (rc != NSX_OK) return rc;
+  return nsx_create(&p, device, out);
+}
+
+int64_t nsx_dim(const nsx_handle *h) { return h ? h->no_state : 0; }
+int32_t nsx_nblocks(const nsx_handle *h) { return h ? (int32_t)h->blocks.size() : 0; }
+
+int nsx_blocks(const nsx_handle *h, int32_t *blocks4, int64_t *offsets) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    for (size_t i = 0; i < h->blocks.size(); ++i) {
+      if (blocks4) {
+        blocks4[4 * i + 0] = h->blocks[i].J2a;
+        blocks4[4 * i + 1] = h->blocks[i].J2b;
+        blocks4[4 * i + 2] = h->blocks[i].da;
+        blocks4[4 * i + 3] = h->blocks[i].db;
+      }
+      if (offsets) offsets[i] = h->blocks[i].off;
+    }
+    if (offsets) offsets[h->blocks.size()] = h->no_state;
+  });
+}
+
+int nsx_lcoef(const nsx_handle *h, uint8_t *mask) {
+  return guarded([&] {
+    if (!h || !mask) fail(NSX_E_ARG, "null argument");
+    std::memcpy(mask, h->lcoef.data(), h->lcoef.size());
+  });
+}
+
+double nsx_matvec_flops(const nsx_handle *h) {
+  return h ? h->flops_like + h->flops_y + h->flops_mix + h->flops_a : 0.0;
+}
+
+int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, void *stream) {
+  return guarded([&] {
+    if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
+    if (x == y) fail(NSX_E_ARG, "x and y must not alias");
+    NSX_CUDA(cudaSetDevice(h->device));
+    matvec_device(h, x, y, precision, (cudaStream_t)stream);
+  });
+}
+
+int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision) {
+  return guarded([&] {
+    if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
+    NSX_CUDA(cudaSetDevice(h->device));
+    size_t bytes = sizeof(double) * h->no_state;
+    NSX_CUDA(cudaMemcpy(h->d.xin, x, bytes, cudaMemcpyHostToDevice));
+    matvec_device(h, h->d.xin, h->d.xout, precision, 0);
+    NSX_CUDA(cudaMemcpy(y, h->d.xout, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs, nsx_report *report) {
+  return guarded([&] {
+    if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
+    NSX_CUDA(cudaSetDevice(h->device));
+    solve(h, params, evals, evecs, report);
+  });
+}
+
+void nsx_destroy(nsx_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  release(h);
+  delete h;
+}
+
+}  // extern "C"

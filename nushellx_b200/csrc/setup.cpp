@@ -1,0 +1,358 @@
+// Host-side setup of one J-scheme pn problem (the B200 counterpart of the
+// reference's Lnz_TRD + drdbh, src/NuLnz/NuCoreX.f90:807-1367 and 1428-1577):
+// species tables, the block list and parity mask, the Racah-weighted pn
+// interaction table, and the task lists of the three H.v stages.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include "nsx_internal.h"
+
+namespace nsx {
+
+uint64_t pack_key(int b0, int b1, int b2, int b3, int b4) {
+  return (uint64_t)(uint8_t)b0 | ((uint64_t)(uint8_t)b1 << 8) | ((uint64_t)(uint8_t)b2 << 16) |
+         ((uint64_t)(uint8_t)b3 << 24) | ((uint64_t)(uint8_t)b4 << 32);
+}
+
+int SpeciesPlan::find_key(int J2l, int J2r, int sl, int sr, int lam) const {
+  auto it = key_index.find(pack_key(J2l, J2r, sl, sr, lam));
+  return it == key_index.end() ? -1 : it->second;
+}
+
+// ---- angular momentum (twice-values), Racah's closed forms -------------------
+static double fact_half(int n2) {  // (n2/2)!
+  static std::vector<double> tab;
+  if (tab.empty()) {
+    tab.resize(171);
+    tab[0] = 1.0;
+    for (int i = 1; i < 171; ++i) tab[i] = tab[i - 1] * i;
+  }
+  int n = n2 / 2;
+  if (n < 0 || n > 170) fail(NSX_E_ARG, "angular momentum too large for the factorial table");
+  return tab[n];
+}
+static bool tri(int a, int b, int c) { return std::abs(a - b) <= c && c <= a + b && ((a + b + c) % 2 == 0); }
+static double delta(int a, int b, int c) {
+  return fact_half(a + b - c) * fact_half(a - b + c) * fact_half(-a + b + c) / fact_half(a + b + c + 2);
+}
+// Wigner 6-j {a b c; d e f}, Racah formula (Edmonds 6.3.7).
+double sixj(int a, int b, int c, int d, int e, int f) {
+  if (!tri(a, b, c) || !tri(a, e, f) || !tri(d, b, f) || !tri(d, e, c)) return 0.0;
+  double pre = std::sqrt(delta(a, b, c) * delta(a, e, f) * delta(d, b, f) * delta(d, e, c));
+  int tlo = std::max(std::max(a + b + c, a + e + f), std::max(d + b + f, d + e + c));
+  int thi = std::min(std::min(a + b + d + e, b + c + e + f), a + c + d + f);
+  double s = 0.0;
+  for (int t = tlo; t <= thi; t += 2) {
+    double num = ((t / 2) % 2 ? -1.0 : 1.0) * fact_half(t + 2);
+    double den = fact_half(t - a - b - c) * fact_half(t - a - e - f) * fact_half(t - d - b - f) *
+                 fact_half(t - d - e - c) * fact_half(a + b + d + e - t) * fact_half(b + c + e + f - t) *
+                 fact_half(a + c + d + f - t);
+    s += num / den;
+  }
+  return pre * s;
+}
+// W(j1 j2 j3 j4; J K) = (-1)^((j1+j2+j3+j4)/2) {j1 j2 J; j4 j3 K}  (src/NuCommon/NuCommon.f90:3255-3265)
+double racah_w(int j1, int j2, int j3, int j4, int J, int K) {
+  double ph = (((j1 + j2 + j3 + j4) / 2) % 2) ? -1.0 : 1.0;
+  return ph * sixj(j1, j2, J, j4, j3, K);
+}
+// (-1)^((Jal+Jbr-J-lam)/2) W(Jal Jbl Jar Jbr; J lam) sqrt(lam+1)  (src/NuLnz/NuCoreX.f90:1114-1126)
+static double racah_weight(int Jal, int Jbl, int Jar, int Jbr, int J, int lam) {
+  double w = racah_w(Jal, Jbl, Jar, Jbr, J, lam);
+  if (w == 0.0) return 0.0;
+  int e = (Jal + Jbr - J - lam) / 2;
+  double ph = (e % 2) ? -1.0 : 1.0;
+  return ph * w * std::sqrt((double)lam + 1.0);
+}
+
+// ---- species ------------------------------------------------------------------
+static void load_species(SpeciesPlan &S, const nsx_species &s, const char *name) {
+  if (s.nspart <= 0 || s.maxJ2 < s.minJ2 || ((s.maxJ2 - s.minJ2) % 2) != 0)
+    fail(NSX_E_ARG, std::string("species ") + name + ": bad partition count or J range");
+  S.nspart = s.nspart;
+  S.minJ2 = s.minJ2;
+  S.maxJ2 = s.maxJ2;
+  S.nJ = (s.maxJ2 - s.minJ2) / 2 + 1;
+  S.shell_first = s.shell_first;
+  S.nshell = s.nshell;
+  S.njt.assign(s.njt, s.njt + (size_t)S.nJ * S.nspart);
+  S.par.assign(s.parity, s.parity + S.nspart);
+  for (int v : S.njt)
+    if (v < 0) fail(NSX_E_ARG, std::string("species ") + name + ": negative nJT");
+  S.poff.assign(S.nJ, std::vector<int>(S.nspart + 1, 0));
+  for (int j = 0; j < S.nJ; ++j)
+    for (int p = 0; p < S.nspart; ++p) S.poff[j][p + 1] = S.poff[j][p] + S.njt[(size_t)j * S.nspart + p];
+  // densities: walk the masks in .trd order (src/NuCommonX/NuCommonX.f90:609-636 next_ij)
+  S.keys.resize(s.nkeys);
+  S.kblocks.assign(s.nkeys, {});
+  int64_t nvals = s.nkeys ? s.val_off[s.nkeys] : 0;
+  S.vals.assign(s.vals, s.vals + nvals);
+  for (int k = 0; k < s.nkeys; ++k) {
+    const uint8_t *kb = s.keys + 8 * (size_t)k;
+    uint64_t key = pack_key(kb[0], kb[1], kb[2], kb[3], kb[4]);
+    S.keys[k] = key;
+    S.key_index[key] = k;
+    int J2l = kb[0], J2r = kb[1];
+    int64_t v = s.val_off[k];
+    for (int r = 0; r < S.nspart; ++r) {
+      const uint32_t *m = s.masks + ((size_t)k * S.nspart + r) * s.words;
+      for (int l = 0; l < S.nspart; ++l) {
+        if (!((m[l / 32] >> (l % 32)) & 1u)) continue;
+        int nl = S.njt_of(l, J2l), nr = S.njt_of(r, J2r);
+        if (nl == 0 || nr == 0) fail(NSX_E_ARG, std::string("species ") + name + ": density block on an empty partition");
+        S.kblocks[k].push_back({l, r, v});
+        v += (int64_t)nl * nr;
+      }
+    }
+    if (v != s.val_off[k + 1]) fail(NSX_E_ARG, std::string("species ") + name + ": density key size disagrees with its masks");
+  }
+  // like-particle Hamiltonian: dense per J from the symmetric segments
+  S.hoff.assign(S.nJ + 1, 0);
+  for (int j = 0; j < S.nJ; ++j) {
+    int64_t d = S.poff[j][S.nspart];
+    S.hoff[j + 1] = S.hoff[j] + d * d;
+  }
+  S.hdense.assign(S.hoff[S.nJ], 0.0);
+  for (int g = 0; g < s.nseg; ++g) {
+    int J2 = s.seg_J2[g];
+    if (!S.has_J(J2)) fail(NSX_E_ARG, std::string("species ") + name + ": segment J out of range");
+    int j = S.jidx(J2);
+    int np = s.seg_np[g] - 1, npr = s.seg_npr[g] - 1;
+    if (np < 0 || npr < 0 || np >= S.nspart || npr >= S.nspart || npr < np)
+      fail(NSX_E_ARG, std::string("species ") + name + ": bad segment partitions");
+    int nl = S.njt_of(np, J2), nr = S.njt_of(npr, J2);
+    if ((int64_t)nl * nr != s.seg_off[g + 1] - s.seg_off[g]) fail(NSX_E_ARG, std::string("species ") + name + ": segment size mismatch");
+    int64_t d = S.poff[j][S.nspart];
+    double *H = S.hdense.data() + S.hoff[j];
+    const double *M = s.seg_vals + s.seg_off[g];
+    int ro = S.poff[j][np], co = S.poff[j][npr];
+    // matrix(dimptr, dimpt): value[kr + nr*kl] = H[(np,kl), (npr,kr)]
+    for (int kl = 0; kl < nl; ++kl)
+      for (int kr = 0; kr < nr; ++kr) {
+        double v = M[kr + (int64_t)nr * kl];
+        H[(ro + kl) + d * (co + kr)] = v;
+        H[(co + kr) + d * (ro + kl)] = v;
+      }
+  }
+}
+
+void build_plan(nsx_handle *h, const nsx_problem *p) {
+  h->J2 = p->J2;
+  h->parity = p->parity;
+  h->renorm = p->renorm;
+  load_species(h->A, p->a, "a");
+  load_species(h->B, p->b, "b");
+  SpeciesPlan &A = h->A, &B = h->B;
+  // pn multipole interaction (src/NuLnz/NuCoreX.f90:1133-1142: tiny values zeroed, times renorm)
+  for (int i = 0; i < p->nop; ++i) {
+    const uint8_t *kb = p->op_keys + 8 * (size_t)i;
+    double v = p->op_vals[i];
+    if (std::fabs(v) < 1e-10) v = 0.0;
+    h->vop[pack_key(kb[0], kb[1], kb[2], kb[3], kb[4])] = v * p->renorm;
+  }
+  // block list (src/NuLnz/NuCoreX.f90:926-988): ascending (2Ja, 2Jb)
+  const int J2 = p->J2;
+  h->blocks.clear();
+  for (int ja = A.minJ2; ja <= A.maxJ2; ja += 2) {
+    int lo = std::max(std::abs(ja - J2), B.minJ2);
+    int hi = std::min(ja + J2, B.maxJ2);
+    lo += (lo - B.minJ2) % 2;
+    for (int jb = lo; jb <= hi; jb += 2) h->blocks.push_back({ja, jb, A.dim(ja), B.dim(jb), 0});
+  }
+  int64_t off = 0;
+  for (auto &b : h->blocks) {
+    b.off = off;
+    off += (int64_t)b.da * b.db;
+  }
+  h->no_state = off;
+  if (off == 0) fail(NSX_E_ARG, "empty J-scheme space");
+  std::map<std::pair<int, int>, int> bidx;
+  for (size_t i = 0; i < h->blocks.size(); ++i) bidx[{h->blocks[i].J2a, h->blocks[i].J2b}] = (int)i;
+  // parity mask lcoef (src/NuLnz/NuCoreX.f90:996-1030)
+  h->lcoef.assign(off, 0);
+  for (auto &b : h->blocks) {
+    int64_t n = b.off;
+    for (int pb = 0; pb < B.nspart; ++pb)
+      for (int kb = 0; kb < B.njt_of(pb, b.J2b); ++kb)
+        for (int pa = 0; pa < A.nspart; ++pa)
+          for (int ka = 0; ka < A.njt_of(pa, b.J2a); ++ka, ++n)
+            h->lcoef[n] = (p->parity == 0 || A.par[pa] * B.par[pb] == p->parity) ? 1 : 0;
+  }
+  // key indices: a-keys by (Jl, Jr); b-keys by (Jl, Jr, lam)
+  std::map<std::pair<int, int>, std::vector<int>> akeys;
+  std::map<std::tuple<int, int, int>, std::vector<int>> bkeys;
+  for (int k = 0; k < (int)A.keys.size(); ++k) {
+    uint64_t key = A.keys[k];
+    akeys[{(int)(key & 255), (int)((key >> 8) & 255)}].push_back(k);
+  }
+  for (int k = 0; k < (int)B.keys.size(); ++k) {
+    uint64_t key = B.keys[k];
+    bkeys[{(int)(key & 255), (int)((key >> 8) & 255), (int)((key >> 32) & 255)}].push_back(k);
+  }
+  // like-particle tiles and flops (segment count, src/NuCommonX/NuCommonX.f90:1009-1104)
+  h->ltiles.clear();
+  h->flops_like = 0;
+  for (auto &b : h->blocks) {
+    if (b.da == 0 || b.db == 0) continue;
+    for (int r0 = 0; r0 < b.da; r0 += 64)
+      for (int c0 = 0; c0 < b.db; c0 += 64)
+        h->ltiles.push_back({b.off, A.hoff[A.jidx(b.J2a)], B.hoff[B.jidx(b.J2b)], b.da, b.db, r0, c0});
+  }
+  for (int g = 0; g < p->a.nseg; ++g) {
+    int J2s = p->a.seg_J2[g];
+    double nn = (double)(p->a.seg_off[g + 1] - p->a.seg_off[g]) * (p->a.seg_np[g] == p->a.seg_npr[g] ? 1 : 2);
+    for (auto &b : h->blocks)
+      if (b.J2a == J2s) h->flops_like += 2.0 * nn * b.db;
+  }
+  for (int g = 0; g < p->b.nseg; ++g) {
+    int J2s = p->b.seg_J2[g];
+    double nn = (double)(p->b.seg_off[g + 1] - p->b.seg_off[g]) * (p->b.seg_np[g] == p->b.seg_npr[g] ? 1 : 2);
+    for (auto &b : h->blocks)
+      if (b.J2b == J2s) h->flops_like += 2.0 * nn * b.da;
+  }
+
+  // ---- pn table (drdbh, src/NuLnz/NuCoreX.f90:1428-1577) ----------------------
+  // entries per (output block, J_ar, a-key): list of (b-key, input block, weight)
+  struct Entry { int bk, hb; double w; };
+  std::map<std::pair<int, int>, int> ymat;  // (input block, b-key) -> Y matrix index
+  std::vector<std::pair<int, int>> ymats;
+  std::vector<int64_t> yoff;
+  h->weights.clear();
+  h->ygroups.clear();
+  h->yblks.clear();
+  h->atiles.clear();
+  h->acontribs.clear();
+  h->amixes.clear();
+  h->flops_y = h->flops_mix = h->flops_a = 0;
+  int64_t ytot = 0;
+  auto get_ymat = [&](int hb, int bk) {
+    auto it = ymat.find({hb, bk});
+    if (it != ymat.end()) return it->second;
+    int id = (int)ymats.size();
+    ymat[{hb, bk}] = id;
+    ymats.push_back({hb, bk});
+    yoff.push_back(ytot);
+    int J2bl = (int)(B.keys[bk] & 255);
+    ytot += (int64_t)h->blocks[hb].da * B.dim(J2bl);
+    return id;
+  };
+  const int TW = 64;
+  for (size_t bl = 0; bl < h->blocks.size(); ++bl) {
+    const Block &ob = h->blocks[bl];
+    if (ob.da == 0 || ob.db == 0) continue;
+    // contributions per left partition P_l
+    std::vector<std::vector<AContrib>> per_pl(A.nspart);
+    std::vector<std::vector<std::vector<AMix>>> per_pl_mix(A.nspart);
+    for (int jar = A.minJ2; jar <= A.maxJ2; jar += 2) {
+      auto ait = akeys.find({ob.J2a, jar});
+      if (ait == akeys.end()) continue;
+      for (int ak : ait->second) {
+        uint64_t akey = A.keys[ak];
+        int sal = (akey >> 16) & 255, sar = (akey >> 24) & 255, lam = (akey >> 32) & 255;
+        std::vector<Entry> ents;
+        int jbrn = std::max(std::abs(ob.J2b - lam), std::abs(jar - J2));
+        int jbrx = std::min(std::min(ob.J2b + lam, jar + J2), B.maxJ2);
+        for (int jbr = jbrn; jbr <= jbrx; jbr += 2) {
+          if (!B.has_J(jbr)) continue;
+          auto hit = bidx.find({jar, jbr});
+          if (hit == bidx.end()) continue;
+          const Block &ib = h->blocks[hit->second];
+          if (ib.da == 0 || ib.db == 0) continue;
+          double rw = racah_weight(ob.J2a, ob.J2b, jar, jbr, J2, lam);
+          if (rw == 0.0) continue;
+          auto bit = bkeys.find({ob.J2b, jbr, lam});
+          if (bit == bkeys.end()) continue;
+          for (int bk : bit->second) {
+            uint64_t bkey = B.keys[bk];
+            int sbl = (bkey >> 16) & 255, sbr = (bkey >> 24) & 255;
+            auto vit = h->vop.find(pack_key(sal, sar, sbl, sbr, lam));
+            if (vit == h->vop.end() || vit->second == 0.0) continue;
+            if (B.kblocks[bk].empty()) continue;
+            ents.push_back({bk, hit->second, vit->second * rw});
+          }
+        }
+        if (ents.empty() || A.kblocks[ak].empty()) continue;
+        for (const RhoBlk &rb : A.kblocks[ak]) {
+          if (rb.pl >= A.nspart) continue;
+          int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
+          AContrib c;
+          c.rho = rb.voff;
+          c.nr = nr;
+          std::vector<AMix> mx;
+          for (const Entry &e : ents) {
+            int yid = get_ymat(e.hb, e.bk);
+            AMix m;
+            m.y = yoff[yid] + A.poff[A.jidx(jar)][rb.pr];
+            m.ld = h->blocks[e.hb].da;
+            m.wi = (int)h->weights.size();
+            h->weights.push_back(e.w);
+            mx.push_back(m);
+          }
+          per_pl[rb.pl].push_back(c);
+          per_pl_mix[rb.pl].push_back(std::move(mx));
+          h->flops_a += 2.0 * nl * nr * ob.db;
+          h->flops_mix += 2.0 * nr * ob.db * ents.size();
+        }
+      }
+    }
+    for (int pl = 0; pl < A.nspart; ++pl) {
+      int nl = A.njt_of(pl, ob.J2a);
+      if (nl == 0 || per_pl[pl].empty()) continue;
+      int cb = (int)h->acontribs.size();
+      for (size_t i = 0; i < per_pl[pl].size(); ++i) {
+        AContrib c = per_pl[pl][i];
+        c.m_begin = (int)h->amixes.size();
+        for (auto &m : per_pl_mix[pl][i]) h->amixes.push_back(m);
+        c.m_end = (int)h->amixes.size();
+        h->acontribs.push_back(c);
+      }
+      int ce = (int)h->acontribs.size();
+      for (int c0 = 0; c0 < ob.db; c0 += TW) {
+        ATile t;
+        t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
+        t.ld = ob.da;
+        t.nl = nl;
+        t.col0 = c0;
+        t.ncols = std::min(TW, ob.db - c0);
+        t.c_begin = cb;
+        t.c_end = ce;
+        h->atiles.push_back(t);
+      }
+    }
+  }
+  // Y groups: one per (Y matrix, 128-row tile), sharing the matrix's sub-block list
+  for (size_t y = 0; y < ymats.size(); ++y) {
+    int hb = ymats[y].first, bk = ymats[y].second;
+    const Block &ib = h->blocks[hb];
+    int J2bl = (int)(B.keys[bk] & 255), J2br = (int)((B.keys[bk] >> 8) & 255);
+    int b0 = (int)h->yblks.size();
+    double nnz = 0;
+    for (const RhoBlk &rb : B.kblocks[bk]) {
+      YBlk yb;
+      yb.rho = rb.voff;
+      yb.ccol = B.poff[B.jidx(J2br)][rb.pr];
+      yb.ycol = B.poff[B.jidx(J2bl)][rb.pl];
+      yb.nl = B.njt_of(rb.pl, J2bl);
+      yb.nr = B.njt_of(rb.pr, J2br);
+      nnz += (double)yb.nl * yb.nr;
+      h->yblks.push_back(yb);
+    }
+    int b1 = (int)h->yblks.size();
+    h->flops_y += 2.0 * ib.da * nnz;
+    for (int r0 = 0; r0 < ib.da; r0 += 128) h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1});
+  }
+  h->y_elems = ytot;
+  h->max_ynl = h->max_ynr = h->max_anl = h->max_anr = h->max_mix = 0;
+  for (auto &y : h->yblks) {
+    h->max_ynl = std::max(h->max_ynl, y.nl);
+    h->max_ynr = std::max(h->max_ynr, y.nr);
+  }
+  for (auto &t : h->atiles) h->max_anl = std::max(h->max_anl, t.nl);
+  for (auto &c : h->acontribs) {
+    h->max_anr = std::max(h->max_anr, c.nr);
+    h->max_mix = std::max(h->max_mix, c.m_end - c.m_begin);
+  }
+}
+
+}  // namespace nsx

@@ -1,0 +1,254 @@
+"""Python binding of libnsx (ctypes over the C ABI of include/nsx.h).
+
+This mirrors the reference's hot-path interface: a ``Solver`` is what the
+reference's Lnz_TRD sets up (src/NuLnz/NuCoreX.f90:807-1367), ``matvec`` is its
+multiplyx/multiplya/multiplyb sequence (NuCoreX.f90:76-226) and ``solve`` its
+Lnz_OP (NuCoreX.f90:240-751).  The CUDA library is the only implementation:
+if libnsx.so is missing or fails to load, every entry point raises -- there is
+no CPU fallback.
+"""
+import ctypes as C
+import json
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnsx.so")
+
+NSX_FP64 = 0
+NSX_FP32 = 1
+_ERRNAMES = {-1: "NSX_E_ARG", -2: "NSX_E_IO", -3: "NSX_E_CUDA", -4: "NSX_E_NOMEM", -5: "NSX_E_NUMERIC",
+             -6: "NSX_E_NOCONV"}
+
+_p = C.POINTER
+
+
+class Species(C.Structure):
+    _fields_ = [("nspart", C.c_int32), ("minJ2", C.c_int32), ("maxJ2", C.c_int32), ("njt", _p(C.c_int32)),
+                ("parity", _p(C.c_int32)), ("shell_first", C.c_int32), ("nshell", C.c_int32),
+                ("nkeys", C.c_int32), ("keys", _p(C.c_uint8)), ("val_off", _p(C.c_int64)),
+                ("vals", _p(C.c_double)), ("words", C.c_int32), ("masks", _p(C.c_uint32)),
+                ("nseg", C.c_int32), ("seg_J2", _p(C.c_int32)), ("seg_np", _p(C.c_int32)),
+                ("seg_npr", _p(C.c_int32)), ("seg_off", _p(C.c_int64)), ("seg_vals", _p(C.c_double))]
+
+
+class Problem(C.Structure):
+    _fields_ = [("J2", C.c_int32), ("parity", C.c_int32), ("a", Species), ("b", Species), ("nop", C.c_int32),
+                ("op_keys", _p(C.c_uint8)), ("op_vals", _p(C.c_double)), ("renorm", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("nev", C.c_int32), ("max_iter", C.c_int32), ("window", C.c_int32), ("keep", C.c_int32),
+                ("tol", C.c_double), ("precision", C.c_int32), ("pre_iter", C.c_int32), ("seed", C.c_uint64),
+                ("start", _p(C.c_double)), ("refine", C.c_int32)]
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("matvecs", C.c_int32), ("restarts", C.c_int32),
+                ("converged", C.c_int32), ("seconds", C.c_double), ("matvec_seconds", C.c_double),
+                ("residual", C.c_double * 64)]
+
+    def as_dict(self):
+        return {"iterations": self.iterations, "matvecs": self.matvecs, "restarts": self.restarts,
+                "converged": self.converged, "seconds": self.seconds, "matvec_seconds": self.matvec_seconds}
+
+
+class Files(C.Structure):
+    _fields_ = [("a", C.c_char_p), ("b", C.c_char_p), ("inter", C.c_char_p), ("like_a", C.c_char_p),
+                ("like_b", C.c_char_p), ("T2_a", C.c_int32), ("nmp_a", C.c_int32), ("T2_b", C.c_int32),
+                ("nmp_b", C.c_int32), ("xtra", C.c_char), ("J2", C.c_int32), ("parity", C.c_int32),
+                ("nshells", C.c_int32), ("nshells_p", C.c_int32), ("shell_parity", _p(C.c_int32))]
+
+
+SYMBOLS = {
+    "nsx_create": (C.c_int, [_p(Problem), C.c_int, _p(C.c_void_p)]),
+    "nsx_load_files": (C.c_int, [_p(Files), C.c_int, _p(C.c_void_p)]),
+    "nsx_file_code": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p]),
+    "nsx_dim": (C.c_int64, [C.c_void_p]),
+    "nsx_nblocks": (C.c_int32, [C.c_void_p]),
+    "nsx_blocks": (C.c_int, [C.c_void_p, _p(C.c_int32), _p(C.c_int64)]),
+    "nsx_lcoef": (C.c_int, [C.c_void_p, _p(C.c_uint8)]),
+    "nsx_matvec_flops": (C.c_double, [C.c_void_p]),
+    "nsx_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
+    "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
+    "nsx_destroy": (None, [C.c_void_p]),
+    "nsx_last_error": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libnsx.so (raises OSError if it is absent: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"libnsx.so not built at {path}: run `python -m nushellx_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SYMBOLS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class NsxError(RuntimeError):
+    def __init__(self, rc, msg):
+        super().__init__(f"{_ERRNAMES.get(rc, rc)}: {msg}")
+        self.rc = rc
+
+
+def _check(rc):
+    if rc != 0:
+        raise NsxError(rc, _lib.nsx_last_error().decode(errors="replace"))
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(_p(ctype)) if a is not None and len(a) else None
+
+
+def _species_struct(keep, S, dens, segs):
+    njt = np.zeros(((S.maxJ2 - S.minJ2) // 2 + 1, len(S.parts)), dtype=np.int32)
+    for ip in range(len(S.parts)):
+        for k in range(njt.shape[0]):
+            njt[k, ip] = S.njt(ip, S.minJ2 + 2 * k)
+    par = np.array(S.part_parity, dtype=np.int32)
+    arrs = dict(njt=njt.ravel(), par=par, keys=dens["keys"], val_off=dens["val_off"],
+                vals=np.ascontiguousarray(dens["vals"], dtype=np.float64),
+                masks=np.ascontiguousarray(dens["masks"].ravel(), dtype=np.uint32),
+                sJ=segs["J2"], snp=segs["np"], snpr=segs["npr"], soff=segs["off"],
+                svals=np.ascontiguousarray(segs["vals"], dtype=np.float64))
+    keep.append(arrs)
+    s = Species()
+    s.nspart, s.minJ2, s.maxJ2 = len(S.parts), S.minJ2, S.maxJ2
+    s.njt = _ptr(arrs["njt"], C.c_int32)
+    s.parity = _ptr(arrs["par"], C.c_int32)
+    s.shell_first = S.shell_offset + 1
+    s.nshell = S.norb
+    s.nkeys = len(arrs["val_off"]) - 1
+    s.keys = _ptr(arrs["keys"], C.c_uint8)
+    s.val_off = _ptr(arrs["val_off"], C.c_int64)
+    s.vals = _ptr(arrs["vals"], C.c_double)
+    s.words = dens["words"]
+    s.masks = _ptr(arrs["masks"], C.c_uint32)
+    s.nseg = len(arrs["sJ"])
+    s.seg_J2 = _ptr(arrs["sJ"], C.c_int32)
+    s.seg_np = _ptr(arrs["snp"], C.c_int32)
+    s.seg_npr = _ptr(arrs["snpr"], C.c_int32)
+    s.seg_off = _ptr(arrs["soff"], C.c_int64)
+    s.seg_vals = _ptr(arrs["svals"], C.c_double)
+    return s
+
+
+class Solver:
+    """One J-scheme problem resident on a GPU."""
+
+    def __init__(self, handle, lib):
+        self._h = handle
+        self._lib = lib
+        self.dim = int(lib.nsx_dim(handle))
+        nb = int(lib.nsx_nblocks(handle))
+        bb = np.zeros(nb * 4, dtype=np.int32)
+        off = np.zeros(nb + 1, dtype=np.int64)
+        _check(lib.nsx_blocks(handle, bb.ctypes.data_as(_p(C.c_int32)), off.ctypes.data_as(_p(C.c_int64))))
+        self.blocks = bb.reshape(nb, 4)
+        self.offsets = off
+        m = np.zeros(self.dim, dtype=np.uint8)
+        _check(lib.nsx_lcoef(handle, m.ctypes.data_as(_p(C.c_uint8))))
+        self.lcoef = m.astype(bool)
+        self.flops = float(lib.nsx_matvec_flops(handle))
+
+    # -- construction --------------------------------------------------------------
+    @classmethod
+    def from_problem(cls, P, device=0):
+        """From an in-memory generated problem (FP64 operator data, no file rounding)."""
+        from .gen.writer import density_arrays, segment_arrays
+        lib = load_library()
+        keep = []
+        prob = Problem()
+        prob.J2, prob.parity = P.J2, P.parity
+        prob.a = _species_struct(keep, P.A, density_arrays(P.A, P.rhoA), segment_arrays(P.A, P.segA))
+        prob.b = _species_struct(keep, P.B, density_arrays(P.B, P.rhoB), segment_arrays(P.B, P.segB))
+        norb = P.space.norb
+        okeys, ovals = [], []
+        for (o1, o3, o2, o4, lam), v in sorted(P.vlam.items()):
+            okeys.append(bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]))
+            ovals.append(v)
+        ok = np.frombuffer(b"".join(okeys), dtype=np.uint8).copy()
+        ov = np.array(ovals, dtype=np.float64)
+        keep.append((ok, ov))
+        prob.nop = len(ovals)
+        prob.op_keys = _ptr(ok, C.c_uint8)
+        prob.op_vals = _ptr(ov, C.c_double)
+        prob.renorm = P.renorm
+        h = C.c_void_p()
+        _check(lib.nsx_create(C.byref(prob), device, C.byref(h)))
+        return cls(h, lib)
+
+    @classmethod
+    def from_files(cls, manifest, device=0):
+        """From the reference-format files described by a generator manifest (dict or .json path)."""
+        lib = load_library()
+        if isinstance(manifest, str):
+            with open(manifest) as f:
+                manifest = json.load(f)
+        m = manifest
+        sp = np.array(m["shell_parity"], dtype=np.int32)
+        f = Files()
+        f.a, f.b, f.inter = m["a"].encode(), m["b"].encode(), m["int"].encode()
+        f.like_a, f.like_b = m["like_a"].encode(), m["like_b"].encode()
+        f.T2_a, f.nmp_a, f.T2_b, f.nmp_b = m["nprot"], -m["nprot"], m["nneut"], m["nneut"]
+        f.xtra = b"x"
+        f.J2, f.parity = m["J2"], m["parity"]
+        f.nshells, f.nshells_p = 2 * m["norb"], m["norb"]
+        f.shell_parity = sp.ctypes.data_as(_p(C.c_int32))
+        h = C.c_void_p()
+        _check(lib.nsx_load_files(C.byref(f), device, C.byref(h)))
+        return cls(h, lib)
+
+    # -- operations -----------------------------------------------------------------
+    def matvec_host(self, x, precision=NSX_FP64):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert x.shape == (self.dim,)
+        y = np.empty_like(x)
+        _check(self._lib.nsx_matvec_host(self._h, x.ctypes.data_as(_p(C.c_double)),
+                                         y.ctypes.data_as(_p(C.c_double)), precision))
+        return y
+
+    def matvec(self, x_ptr, y_ptr, precision=NSX_FP64, stream=None):
+        """Device pointers (e.g. torch tensor .data_ptr()); stream is a cudaStream_t integer or None."""
+        _check(self._lib.nsx_matvec(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), precision,
+                                    C.c_void_p(stream) if stream else None))
+
+    def solve(self, nev=10, tol=1e-6, precision=NSX_FP64, window=100, keep=0, max_iter=3000, pre_iter=2,
+              seed=5, start=None, refine=False, want_vectors=False):
+        p = Params()
+        p.nev, p.tol, p.precision, p.window, p.keep = nev, tol, precision, window, keep
+        p.max_iter, p.pre_iter, p.seed, p.refine = max_iter, pre_iter, seed, int(bool(refine))
+        st = None
+        if start is not None:
+            st = np.ascontiguousarray(start, dtype=np.float64)
+            p.start = st.ctypes.data_as(_p(C.c_double))
+        ev = np.zeros(nev)
+        vecs = np.zeros((nev, self.dim)) if want_vectors else None
+        rep = Report()
+        _check(self._lib.nsx_solve(self._h, C.byref(p), ev.ctypes.data_as(_p(C.c_double)),
+                                   vecs.ctypes.data_as(_p(C.c_double)) if vecs is not None else None,
+                                   C.byref(rep)))
+        out = rep.as_dict()
+        out["residual"] = [rep.residual[i] for i in range(min(nev, 64))]
+        return ev, vecs, out
+
+    def close(self):
+        if self._h:
+            self._lib.nsx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
