@@ -354,7 +354,8 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   ensure_precision(h, prec);
 
   Workspace ws;
-  NSX_CUDA(cudaMalloc(&ws.V, sizeof(double) * n * (m + 1)));
+  // basis (m+1 vectors); the FP64 refinement reuses it for 2*nev rotated vectors
+  NSX_CUDA(cudaMalloc(&ws.V, sizeof(double) * n * std::max(m + 1, 2 * nev)));
   NSX_CUDA(cudaMalloc(&ws.w, sizeof(double) * n));
   NSX_CUDA(cudaMalloc(&ws.tmp, sizeof(double) * n * std::max(keep, nev)));
   NSX_CUDA(cudaMalloc(&ws.partial, sizeof(double) * RED_CTAS * JT));

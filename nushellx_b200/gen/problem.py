@@ -23,11 +23,18 @@ class JProblem:
         self.parity = parity
         self.renorm = renorm
         self.A = Species(space.j2, space.parity, space.spe, nprot, shell_offset=0)
-        self.B = Species(space.j2, space.parity, space.spe, nneut, shell_offset=space.norb)
         self.rhoA = self.A.densities(lam_max)
-        self.rhoB = self.B.densities(lam_max)
         self.segA = self.A.hamiltonian_segments(inter, renorm)
-        self.segB = self.B.hamiltonian_segments(inter, renorm)
+        if nneut == nprot:
+            # same orbits and interaction for both species: share the work, shift the shell numbers
+            import copy
+            self.B = copy.copy(self.A)
+            self.B.shell_offset = space.norb
+            self.rhoB, self.segB = self.rhoA, self.segA
+        else:
+            self.B = Species(space.j2, space.parity, space.spe, nneut, shell_offset=space.norb)
+            self.rhoB = self.B.densities(lam_max)
+            self.segB = self.B.hamiltonian_segments(inter, renorm)
         self.vlam = multipole_pn(inter)
         self._blocks()
 
