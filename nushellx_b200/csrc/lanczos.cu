@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) k_rotate(const double *__restrict__ V, in
 // lda = m).  Tournament (round-robin) ordering: each round rotates m/2 disjoint
 // (p, q) pairs, rows first, then columns.  Outputs eigenvalues (unsorted) in
 // evals and eigenvectors as columns of Vout.  Sweeps stop when the off-diagonal
-// Frobenius norm falls below 1e-15 of the total, at most 60 sweeps; status[0]
+// Frobenius norm falls below 1e-13 of the total, at most 60 sweeps; status[0]
 // = sweeps used, or -1 if not converged (the host reports NSX_E_NUMERIC).
 __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, int m, double *__restrict__ evals,
                                                 double *__restrict__ Vout, int *__restrict__ status) {
@@ -173,17 +173,17 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
       atomicAdd(&totn, lt);
     }
     __syncthreads();
-    if (offn <= 1e-30 * totn || totn == 0.0) break;
+    if (offn <= 1e-26 * totn || totn == 0.0) break;
     __syncthreads();
     for (int round = 0; round < mp - 1; ++round) {
-      // pairs (perm[2i], perm[2i+1])
+      // circle-method pairs (perm[i], perm[mp-1-i]): every pair once per sweep
       for (int i = threadIdx.x; i < mp / 2; i += blockDim.x) {
-        int p = perm[2 * i], q = perm[2 * i + 1];
+        int p = perm[i], q = perm[mp - 1 - i];
         if (p > q) { int t = p; p = q; q = t; }
         double apq = A[p + mp * q];
         double c = 1.0, s = 0.0;
-        if (apq != 0.0) {
-          double app = A[p + mp * p], aqq = A[q + mp * q];
+        double app = A[p + mp * p], aqq = A[q + mp * q];
+        if (fabs(apq) > 1e-18 * (fabs(app) + fabs(aqq)) && apq != 0.0) {
           double tau = (aqq - app) / (2.0 * apq);
           double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
           c = 1.0 / sqrt(1.0 + t * t);
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
       // rows: A <- J^T A
       for (int e = threadIdx.x; e < (mp / 2) * mp; e += blockDim.x) {
         int i = e / mp, k = e % mp;
-        int p = perm[2 * i], q = perm[2 * i + 1];
+        int p = perm[i], q = perm[mp - 1 - i];
         if (p > q) { int t = p; p = q; q = t; }
         double c = cs[i], s = sn[i];
         double ap = A[p + mp * k], aq = A[q + mp * k];
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
       // columns: A <- A J ; Q <- Q J
       for (int e = threadIdx.x; e < (mp / 2) * mp; e += blockDim.x) {
         int i = e / mp, k = e % mp;
-        int p = perm[2 * i], q = perm[2 * i + 1];
+        int p = perm[i], q = perm[mp - 1 - i];
         if (p > q) { int t = p; p = q; q = t; }
         double c = cs[i], s = sn[i];
         double ap = A[k + mp * p], aq = A[k + mp * q];
