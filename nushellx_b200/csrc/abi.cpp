@@ -142,6 +142,36 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
   });
 }
 
+int nsx_stats_reset(nsx_handle *h, int32_t timing) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    flush_stage_events(h);
+    h->launches = h->matvecs = 0;
+    for (int i = 0; i < 4; ++i) {
+      h->stage_launches[i] = 0;
+      h->stage_ms[i] = 0;
+    }
+    h->timing = timing != 0;
+  });
+}
+
+int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
+  return guarded([&] {
+    if (!h || !out) fail(NSX_E_ARG, "null argument");
+    NSX_CUDA(cudaSetDevice(h->device));
+    flush_stage_events(h);
+    out->launches = h->launches;
+    out->matvecs = h->matvecs;
+    // algorithmic figures for the precision of the last H.v
+    int prec = h->last_precision;
+    stage_bytes_flops(h, prec, out->stage_bytes, out->stage_flops);
+    for (int i = 0; i < 4; ++i) {
+      out->stage_launches[i] = h->stage_launches[i];
+      out->stage_ms[i] = h->stage_ms[i];
+    }
+  });
+}
+
 void nsx_destroy(nsx_handle *h) {
   if (!h) return;
   cudaSetDevice(h->device);

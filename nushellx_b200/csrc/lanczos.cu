@@ -28,6 +28,10 @@
 namespace nsx {
 
 static constexpr int RED_CTAS = 592;   // 148 SMs x 4
+static thread_local int64_t *g_launches = nullptr;  // the solving handle's launch counter
+static inline void count_launch() {
+  if (g_launches) ++*g_launches;
+}
 static constexpr int JT = 8;           // vectors per pass of the dot kernel
 
 __device__ __forceinline__ uint64_t splitmix(uint64_t z) {
@@ -255,13 +259,16 @@ static void dots(Workspace &ws, const double *V, int64_t ld, int cnt, const doub
                  bool acc, cudaStream_t s) {
   for (int j0 = 0; j0 < cnt; j0 += JT) {
     int c = std::min(JT, cnt - j0);
+    count_launch();
     k_dots<<<RED_CTAS, 256, 0, s>>>(V, ld, j0, c, w, n, ws.partial);
+    count_launch();
     k_dots_reduce<<<1, 32 * JT, 0, s>>>(ws.partial, RED_CTAS, c, h, j0, acc ? 1 : 0);
   }
 }
 static void subtract(const double *V, int64_t ld, int cnt, const double *h, double *w, int64_t n, cudaStream_t s) {
   for (int j0 = 0; j0 < cnt; j0 += 256) {
     int c = std::min(256, cnt - j0);
+    count_launch();
     k_sub<<<grid_for(n), 256, 0, s>>>(V + (int64_t)j0 * ld, ld, c, h + j0, w, n);
   }
 }
@@ -272,6 +279,7 @@ static void jacobi(Workspace &ws, int m, const std::vector<double> &T, std::vect
   int mp = m + (m & 1);
   size_t smem = sizeof(double) * (2 * (size_t)mp * mp + mp) + sizeof(int) * mp;
   NSX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  count_launch();
   k_jacobi<<<1, 512, smem, s>>>(ws.T, m, ws.ev, ws.S, ws.status);
   NSX_CUDA(cudaGetLastError());
   std::vector<double> e(m), q((size_t)m * m);
@@ -352,6 +360,10 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   const int prec = P->precision;
   cudaStream_t s = 0;
   ensure_precision(h, prec);
+  struct CounterScope {
+    CounterScope(int64_t *p) { g_launches = p; }
+    ~CounterScope() { g_launches = nullptr; }
+  } counter_scope(&h->launches);
 
   Workspace ws;
   // basis (m+1 vectors); the FP64 refinement reuses it for 2*nev rotated vectors
@@ -375,15 +387,18 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   if (P->start) {
     NSX_CUDA(cudaMemcpy(V(0), P->start, sizeof(double) * n, cudaMemcpyHostToDevice));
   } else {
+    count_launch();
     k_rand<<<grid_for(n), 256, 0, s>>>(V(0), ws.mask, n, P->seed ? P->seed : 5);
   }
   double nn = host_norm2(ws, V(0), n, s);
   if (!(nn > 0) || !std::isfinite(nn)) fail(NSX_E_ARG, "start vector is zero or not finite");
+  count_launch();
   k_scale<<<grid_for(n), 256, 0, s>>>(V(0), V(0), ws.h2, n);
   for (int it = 0; it < P->pre_iter; ++it) {  // power pre-iterations (NuCoreX.f90:639-654)
     tm.matvec(V(0), ws.w, prec, s);
     ++matvecs;
     dots(ws, ws.w, 0, 1, ws.w, n, ws.h2, false, s);
+    count_launch();
     k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(0), ws.h2, n);
   }
   NSX_CUDA(cudaGetLastError());
@@ -420,6 +435,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     const bool limit = iters >= max_iter;
     if (!exhausted && !full && beta <= 1e-7 * std::max(scale, 1.0)) {
       // breakdown: a random direction orthogonal to the basis, zero coupling (NuCoreX.f90:368-382)
+      count_launch();
       k_rand<<<grid_for(n), 256, 0, s>>>(ws.w, ws.mask, n, 0xA5A5A5A5ull + (uint64_t)iters);
       for (int pass = 0; pass < 2; ++pass) {
         dots(ws, ws.V, n, i + 1, ws.w, n, ws.h, false, s);
@@ -429,6 +445,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
       beta = 0.0;
     }
     if (!full && !exhausted) {
+      count_launch();
       k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(i + 1), ws.h2 + (i + 1), n);
       NSX_CUDA(cudaGetLastError());
       T[(i + 1) + (size_t)m * i] = beta;
@@ -460,6 +477,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
       size_t smem = sizeof(double) * mm * nev;
       NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)std::max<size_t>(smem, 1024)));
+      count_launch();
       k_rotate<<<grid_for(n), 256, smem, s>>>(ws.V, n, mm, ws.S, nev, ws.tmp, n);
       NSX_CUDA(cudaGetLastError());
       break;
@@ -477,8 +495,10 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     size_t smem = sizeof(double) * m * keep;
     NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)std::max<size_t>(smem, 1024)));
+    count_launch();
     k_rotate<<<grid_for(n), 256, smem, s>>>(ws.V, n, m, ws.S, keep, ws.tmp, n);
     NSX_CUDA(cudaMemcpyAsync(ws.V, ws.tmp, sizeof(double) * n * keep, cudaMemcpyDeviceToDevice, s));
+    count_launch();
     k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(keep), ws.h2 + (i + 1), n);
     NSX_CUDA(cudaGetLastError());
     std::fill(T.begin(), T.end(), 0.0);
@@ -517,7 +537,9 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     NSX_CUDA(cudaMemcpyAsync(ws.S, S2.data(), sizeof(double) * nev * nev, cudaMemcpyHostToDevice, s));
     size_t smem = sizeof(double) * nev * nev;
     NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1024)));
+    count_launch();
     k_rotate<<<grid_for(n), 256, smem, s>>>(ws.tmp, n, nev, ws.S, nev, ws.V, n);
+    count_launch();
     k_rotate<<<grid_for(n), 256, smem, s>>>(HY, n, nev, ws.S, nev, ws.V + (int64_t)nev * n, n);
     NSX_CUDA(cudaMemcpyAsync(ws.tmp, ws.V, sizeof(double) * n * nev, cudaMemcpyDeviceToDevice, s));
     for (int c = 0; c < nev; ++c) {

@@ -281,31 +281,98 @@ void ensure_precision(nsx_handle *h, int precision) {
   }
 }
 
+// Brackets one stage launch with events when per-stage timing is enabled.
+struct StageScope {
+  nsx_handle *h;
+  int stage;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr, b = nullptr;
+  StageScope(nsx_handle *h_, int st, cudaStream_t s_) : h(h_), stage(st), s(s_) {
+    h->launches++;
+    h->stage_launches[stage]++;
+    if (h->timing) {
+      NSX_CUDA(cudaEventCreate(&a));
+      NSX_CUDA(cudaEventCreate(&b));
+      NSX_CUDA(cudaEventRecord(a, s));
+    }
+  }
+  ~StageScope() {
+    if (h->timing) {
+      cudaEventRecord(b, s);
+      h->stage_events.push_back({stage, {a, b}});
+    }
+  }
+};
+
+void flush_stage_events(nsx_handle *h) {
+  for (auto &e : h->stage_events) {
+    float ms = 0;
+    NSX_CUDA(cudaEventSynchronize(e.second.second));
+    NSX_CUDA(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
+    h->stage_ms[e.first] += ms;
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
+  h->stage_events.clear();
+}
+
+// Algorithmic traffic (each operand read once, each result written once) and
+// flops of one launch of each stage.
+void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]) {
+  const double es = precision == NSX_FP64 ? 8.0 : 4.0;
+  const double n = (double)h->no_state;
+  double rhoA = (double)h->A.vals.size(), rhoB = (double)h->B.vals.size();
+  double hd = (double)(h->A.hdense.size() + h->B.hdense.size());
+  bytes[0] = es * (2.0 * n + hd);                               // C in, out written, dense H
+  bytes[1] = es * (n + rhoB + (double)h->y_elems);              // C in, rho_B, Y written
+  bytes[2] = es * ((double)h->y_elems + rhoA + 2.0 * n) + 4.0 * (double)h->weights.size();  // Y, rho_A, out r/w
+  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);     // one conversion launch
+  flops[0] = h->flops_like;
+  flops[1] = h->flops_y;
+  flops[2] = h->flops_mix + h->flops_a;
+  flops[3] = 0.0;
+}
+
 template <typename T>
 static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T *rhoB, const T *hA, const T *hB,
                        const T *w, T *Y, cudaStream_t s) {
   auto &d = h->d;
-  if (!h->ltiles.empty()) k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
-  if (!h->ygroups.empty())
+  if (!h->ltiles.empty()) {
+    StageScope sc(h, 0, s);
+    k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
+  }
+  if (!h->ygroups.empty()) {
+    StageScope sc(h, 1, s);
     k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
                                                                              h->max_ynr, h->max_ynl);
-  if (!h->atiles.empty())
+  }
+  if (!h->atiles.empty()) {
+    StageScope sc(h, 2, s);
     k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(
         d.atiles, d.acontribs, d.amixes, w, rhoA, Y, out, h->max_anr, h->max_anl, h->max_mix);
+  }
   NSX_CUDA(cudaGetLastError());
 }
 
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s) {
   ensure_precision(h, precision);
   auto &d = h->d;
+  h->matvecs++;
+  h->last_precision = precision;
   if (precision == NSX_FP64) {
     run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.y64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
-    k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
+    {
+      StageScope sc(h, 3, s);
+      k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
+    }
     run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.y32, s);
-    k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
+    {
+      StageScope sc(h, 3, s);
+      k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
+    }
     NSX_CUDA(cudaGetLastError());
   }
 }
@@ -317,6 +384,11 @@ void release(nsx_handle *h) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceBuffers();
+  for (auto &e : h->stage_events) {
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
+  h->stage_events.clear();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   h->ev0 = h->ev1 = nullptr;

@@ -135,6 +135,13 @@ struct nsx_handle {
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // statistics
+  int64_t launches = 0, matvecs = 0;
+  int64_t stage_launches[4] = {0, 0, 0, 0};
+  double stage_ms[4] = {0, 0, 0, 0};
+  bool timing = false;
+  int last_precision = NSX_FP64;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
 };
 
 namespace nsx {
@@ -143,6 +150,8 @@ void upload(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);
+void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]);
+void flush_stage_events(nsx_handle *h);
 double sixj(int a, int b, int c, int d, int e, int f);
 double racah_w(int j1, int j2, int j3, int j4, int J, int K);
 }  // namespace nsx

@@ -296,6 +296,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
         }
       }
     }
+    std::vector<ATile> btiles;  // this output block's tiles, reordered below
     for (int pl = 0; pl < A.nspart; ++pl) {
       int nl = A.njt_of(pl, ob.J2a);
       if (nl == 0 || per_pl[pl].empty()) continue;
@@ -317,9 +318,14 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
         t.ncols = std::min(TW, ob.db - c0);
         t.c_begin = cb;
         t.c_end = ce;
-        h->atiles.push_back(t);
+        btiles.push_back(t);
       }
     }
+    // Tiles of the same column range are launched next to each other: they mix the same
+    // Y column slabs (all proton rows P_r) in the same contribution order, so their reads
+    // meet in L2 instead of each going to DRAM.
+    std::stable_sort(btiles.begin(), btiles.end(), [](const ATile &x, const ATile &y) { return x.col0 < y.col0; });
+    h->atiles.insert(h->atiles.end(), btiles.begin(), btiles.end());
   }
   // Y groups: one per (Y matrix, 128-row tile), sharing the matrix's sub-block list
   for (size_t y = 0; y < ymats.size(); ++y) {

@@ -53,6 +53,19 @@ class Report(C.Structure):
                 "converged": self.converged, "seconds": self.seconds, "matvec_seconds": self.matvec_seconds}
 
 
+class Stats(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("matvecs", C.c_int64), ("stage_launches", C.c_int64 * 4),
+                ("stage_ms", C.c_double * 4), ("stage_bytes", C.c_double * 4), ("stage_flops", C.c_double * 4)]
+
+    STAGES = ("k_like", "k_y", "k_a", "k_convert")
+
+    def as_dict(self):
+        return {"launches": self.launches, "matvecs": self.matvecs,
+                "stages": {n: {"launches": self.stage_launches[i], "ms": self.stage_ms[i],
+                               "bytes": self.stage_bytes[i], "flops": self.stage_flops[i]}
+                           for i, n in enumerate(self.STAGES)}}
+
+
 class Files(C.Structure):
     _fields_ = [("a", C.c_char_p), ("b", C.c_char_p), ("inter", C.c_char_p), ("like_a", C.c_char_p),
                 ("like_b", C.c_char_p), ("T2_a", C.c_int32), ("nmp_a", C.c_int32), ("T2_b", C.c_int32),
@@ -72,6 +85,8 @@ SYMBOLS = {
     "nsx_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
+    "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
     "nsx_destroy": (None, [C.c_void_p]),
     "nsx_last_error": (C.c_char_p, []),
 }
@@ -143,6 +158,29 @@ def _species_struct(keep, S, dens, segs):
     return s
 
 
+def build_problem_struct(P):
+    """nsx_problem for an in-memory generated problem; returns (struct, arrays to keep alive)."""
+    from .gen.writer import density_arrays, segment_arrays
+    keep = []
+    prob = Problem()
+    prob.J2, prob.parity = P.J2, P.parity
+    prob.a = _species_struct(keep, P.A, density_arrays(P.A, P.rhoA), segment_arrays(P.A, P.segA))
+    prob.b = _species_struct(keep, P.B, density_arrays(P.B, P.rhoB), segment_arrays(P.B, P.segB))
+    norb = P.space.norb
+    okeys, ovals = [], []
+    for (o1, o3, o2, o4, lam), v in sorted(P.vlam.items()):
+        okeys.append(bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]))
+        ovals.append(v)
+    ok = np.frombuffer(b"".join(okeys), dtype=np.uint8).copy()
+    ov = np.array(ovals, dtype=np.float64)
+    keep.append((ok, ov))
+    prob.nop = len(ovals)
+    prob.op_keys = _ptr(ok, C.c_uint8)
+    prob.op_vals = _ptr(ov, C.c_double)
+    prob.renorm = P.renorm
+    return prob, keep
+
+
 class Solver:
     """One J-scheme problem resident on a GPU."""
 
@@ -165,25 +203,8 @@ class Solver:
     @classmethod
     def from_problem(cls, P, device=0):
         """From an in-memory generated problem (FP64 operator data, no file rounding)."""
-        from .gen.writer import density_arrays, segment_arrays
         lib = load_library()
-        keep = []
-        prob = Problem()
-        prob.J2, prob.parity = P.J2, P.parity
-        prob.a = _species_struct(keep, P.A, density_arrays(P.A, P.rhoA), segment_arrays(P.A, P.segA))
-        prob.b = _species_struct(keep, P.B, density_arrays(P.B, P.rhoB), segment_arrays(P.B, P.segB))
-        norb = P.space.norb
-        okeys, ovals = [], []
-        for (o1, o3, o2, o4, lam), v in sorted(P.vlam.items()):
-            okeys.append(bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]))
-            ovals.append(v)
-        ok = np.frombuffer(b"".join(okeys), dtype=np.uint8).copy()
-        ov = np.array(ovals, dtype=np.float64)
-        keep.append((ok, ov))
-        prob.nop = len(ovals)
-        prob.op_keys = _ptr(ok, C.c_uint8)
-        prob.op_vals = _ptr(ov, C.c_double)
-        prob.renorm = P.renorm
+        prob, keep = build_problem_struct(P)
         h = C.c_void_p()
         _check(lib.nsx_create(C.byref(prob), device, C.byref(h)))
         return cls(h, lib)
@@ -241,6 +262,14 @@ class Solver:
         out = rep.as_dict()
         out["residual"] = [rep.residual[i] for i in range(min(nev, 64))]
         return ev, vecs, out
+
+    def stats_reset(self, timing=False):
+        _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))
+
+    def stats(self):
+        st = Stats()
+        _check(self._lib.nsx_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
 
     def close(self):
         if self._h:

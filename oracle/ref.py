@@ -1,0 +1,61 @@
+"""ctypes binding of oracle/libnsxref.so (the C restatement of the reference;
+test infrastructure and host-core baseline only)."""
+import ctypes as C
+import os
+import numpy as np
+
+from .build_ref import build, LIB
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        L.ref_create.restype = C.c_void_p
+        L.ref_create.argtypes = [C.c_void_p]
+        L.ref_dim.restype = C.c_int64
+        L.ref_dim.argtypes = [C.c_void_p]
+        L.ref_nthreads.restype = C.c_int
+        L.ref_nthreads.argtypes = [C.c_void_p]
+        L.ref_matvec.restype = None
+        L.ref_matvec.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.ref_lanczos.restype = C.c_double
+        L.ref_lanczos.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_destroy.restype = None
+        L.ref_destroy.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class RefSolver:
+    """The reference algorithm (FP32 storage, axpy order, OpenMP) on a generated problem."""
+
+    def __init__(self, P):
+        from nushellx_b200.nsx import build_problem_struct
+        self._prob, self._keep = build_problem_struct(P)
+        self._h = lib().ref_create(C.byref(self._prob))
+        self.dim = int(lib().ref_dim(self._h))
+        self.threads = int(lib().ref_nthreads(self._h))
+
+    def matvec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty_like(x)
+        lib().ref_matvec(self._h, x.ctypes.data_as(C.POINTER(C.c_float)), y.ctypes.data_as(C.POINTER(C.c_float)))
+        return y
+
+    def lanczos(self, npre, nsteps, seed=5):
+        a = np.zeros(max(nsteps, 1))
+        b = np.zeros(max(nsteps, 1))
+        pre = C.c_double(0)
+        t = lib().ref_lanczos(self._h, npre, nsteps, seed, a.ctypes.data_as(C.POINTER(C.c_double)),
+                              b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pre))
+        return t, pre.value, a[:nsteps], b[:nsteps]
+
+    def close(self):
+        if self._h:
+            lib().ref_destroy(self._h)
+            self._h = None
