@@ -149,8 +149,8 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
               nsx_report *report);
 
 /* Device-side statistics of a handle (for benchmarking and profiling).
- * Stages of one H.v: 0 = like-particle GEMMs (k_like), 1 = neutron-side Y
- * products (k_y), 2 = mixing + proton side (k_a), 3 = precision conversion.
+ * Stages of one H.v: 0 = like-particle products (k_like), 1 = fused pn
+ * product (k_pn), 2 = unused, 3 = FP64 <-> FP32 conversions.
  * With timing enabled every stage launch is bracketed by CUDA events on its
  * stream; nsx_get_stats synchronises and sums them. */
 typedef struct nsx_stats {

@@ -3,15 +3,22 @@
 // The reference computes the product as multiplyx (pn), multiplya (pp) and
 // multiplyb (nn) in src/NuLnz/NuCoreX.f90:76-226 with axpy loops over density
 // sub-blocks (src/NuCommonX/NuCommonX.f90:745-919, 1009-1104).  Here it is
-// three stream-ordered kernels, each output element owned by exactly one CTA
-// (no atomics, no per-thread vector copies):
+// two stream-ordered kernels; every output element is owned by one CTA (no
+// global atomics, no per-thread copies of the vector):
 //
 //   k_like : out_b  = H_pp(Ja) C_b + C_b H_nn(Jb)              (dense tiled GEMM)
-//   k_y    : Y_(h,k) = C_h rho_k^T for every (input block h, neutron density k)
-//            that the pn table uses -- computed once and reused by every proton
-//            operator, where the reference recomputes it per proton operator;
-//   k_a    : out[P_l rows] += sum_(a,P_r) rho_a[P_l,P_r] (sum_k w_ak Y_(h,k)[P_r rows])
-//            (mixing of the Y intermediates fused into the operand load).
+//   k_pn   : persistent; a CTA owns the output columns of one neutron partition
+//            Q_l (a chunk of CH states) of one block and, for every (J_ar, lam)
+//            group of the pn table,
+//              stage 1: Y_(h,b)[:, chunk] = C_h[:, Q_r cols] rho_b[chunk, Q_r]^T
+//                       into the CTA's scratch slot (written and read back by the
+//                       same CTA: it stays in L2, ~0.5 MB per CTA in flight);
+//              stage 2: per proton partition P_r (8 rows per warp item) the
+//                       sources are mixed in registers, Z_a = sum w_(a,s) Y_s,
+//                       and out[P_l rows] += rho_a[P_l, P_r] Z_a is accumulated
+//                       in shared memory.
+//            Each Y_(h,b) element is computed once (the reference recomputes the
+//            neutron-side product for every proton operator).
 //
 // Templated on the contraction type: double (the FP64 form) or float (the FP32
 // form, FP64 vectors converted at the boundary).
@@ -82,111 +89,123 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
-// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T.
-template <typename T>
-__global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
-                                           const T *__restrict__ x, const T *__restrict__ rho,
-                                           T *__restrict__ Y, int max_nr, int max_nl) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
-  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
-  const YGroup g = groups[blockIdx.x];
-  const int row = g.row0 + threadIdx.x;
-  const bool active = row < g.m;
-  const T *C = x + g.c_base;
-  T *Yg = Y + g.y_base;
-  for (int bi = g.b_begin; bi < g.b_end; ++bi) {
-    const YBlk b = blks[bi];
-    const int n = b.nl * b.nr;
-    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
-    if (active)
-      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
-    __syncthreads();
-    if (active) {
-      for (int l = 0; l < b.nl; ++l) {
-        T acc = T(0);
-        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
-        Yg[row + (int64_t)g.m * (b.ycol + l)] = acc;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// k_a: one CTA per output tile (block, P_l, <=64 columns); 256 threads own the
-// nl x ncols outputs (idx = tid + 256 q).  Per contribution: Z = sum w Y rows
-// (mixing) in shared memory, then acc += rho_a Z.
-constexpr int AQ = 16;  // outputs per thread: supports nl <= 64 with 64 columns
-struct KaLayout {  // byte offsets of the k_a shared-memory arrays (16-byte aligned)
-  size_t rs, zs, ws, ys, ls, total;
+// k_pn: see the file comment.  512 threads (16 warps), one CTA per SM.
+constexpr int PN_WARPS = 16;
+struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte aligned)
+  size_t out, z, w, sidx, total;
   __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ KaLayout(size_t es, int nl, int nr, int nm) {
-    rs = 0;
-    zs = al(rs + es * (size_t)nl * nr);
-    ws = al(zs + es * (size_t)nr * 64);
-    ys = al(ws + es * (size_t)nm);
-    ls = al(ys + 8 * (size_t)nm);
-    total = al(ls + 4 * (size_t)nm);
+  __host__ __device__ PnLayout(size_t es, int max_dal, int ch) {
+    out = 0;
+    z = al(out + es * (size_t)max_dal * ch);
+    w = al(z + es * (size_t)PN_WARPS * MAXA * 8 * ch);
+    sidx = al(w + es * (size_t)MAXA * MAXS);
+    total = al(sidx + 4 * (size_t)MAXS);
   }
 };
-template <typename T>
-__global__ void __launch_bounds__(256) k_a(const ATile *__restrict__ tiles, const AContrib *__restrict__ contribs,
-                                           const AMix *__restrict__ mixes, const T *__restrict__ wts,
-                                           const T *__restrict__ rho, const T *__restrict__ Y, T *__restrict__ out,
-                                           int max_nr, int max_nl, int max_mix) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  KaLayout L(sizeof(T), max_nl, max_nr, max_mix);
-  T *rs = reinterpret_cast<T *>(smem_raw + L.rs);        // [max_nl*max_nr]
-  T *zs = reinterpret_cast<T *>(smem_raw + L.zs);        // [max_nr][64]
-  T *ws = reinterpret_cast<T *>(smem_raw + L.ws);        // [max_mix]
-  int64_t *ys = reinterpret_cast<int64_t *>(smem_raw + L.ys);  // [max_mix]
-  int *ls = reinterpret_cast<int *>(smem_raw + L.ls);    // [max_mix]
-  const ATile t = tiles[blockIdx.x];
-  const int nl = t.nl, ncols = t.ncols;
-  T acc[AQ];
-#pragma unroll
-  for (int q = 0; q < AQ; ++q) acc[q] = T(0);
-  for (int ci = t.c_begin; ci < t.c_end; ++ci) {
-    const AContrib c = contribs[ci];
-    const int nr = c.nr;
-    const int nm = c.m_end - c.m_begin;
-    for (int e = threadIdx.x; e < nl * nr; e += 256) rs[e] = rho[c.rho + e];
-    for (int e = threadIdx.x; e < nm; e += 256) {
-      const AMix m = mixes[c.m_begin + e];
-      ws[e] = wts[m.wi];
-      ys[e] = m.y;
-      ls[e] = m.ld;
-    }
+
+template <typename T, int CH>
+__global__ void __launch_bounds__(512, 1)
+    k_pn(const PnTask *__restrict__ tasks, int ntasks, const TGroup *__restrict__ tgroups,
+         const Group *__restrict__ groups, const TSrc *__restrict__ tsrcs, const PrWork *__restrict__ prwork,
+         const AOp *__restrict__ aops, const T *__restrict__ W, const T *__restrict__ x,
+         const T *__restrict__ rhoA, const T *__restrict__ rhoB, T *__restrict__ out, T *__restrict__ scratch_all,
+         int64_t slot_elems, int *__restrict__ counter, int max_dal) {
+  constexpr int EPL = (8 * CH) / 32;  // stage-2 elements per lane (8 rows x CH columns)
+  extern __shared__ __align__(16) unsigned char smem[];
+  const PnLayout L(sizeof(T), max_dal, CH);
+  T *out_s = reinterpret_cast<T *>(smem + L.out);   // [max_dal][CH] column-major (ld = d_al)
+  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][8][CH]
+  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] compact weights
+  int *sidx_s = reinterpret_cast<int *>(smem + L.sidx);
+  __shared__ int s_task;
+  T *scratch = scratch_all + (int64_t)blockIdx.x * slot_elems;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (;;) {
+    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
-    for (int e = threadIdx.x; e < nr * ncols; e += 256) {
-      const int k = e % nr, j = e / nr;
-      T z = T(0);
-      for (int m = 0; m < nm; ++m) z = fma(ws[m], Y[ys[m] + k + (int64_t)ls[m] * (t.col0 + j)], z);
-      zs[k * 64 + j] = z;
-    }
+    const int ti = s_task;
     __syncthreads();
+    if (ti >= ntasks) break;
+    const PnTask t = tasks[ti];
+    const int dal = t.d_al, nq = t.nq;
+    for (int e = threadIdx.x; e < dal * CH; e += blockDim.x) out_s[e] = T(0);
+    for (int gi = t.g_begin; gi < t.g_end; ++gi) {
+      const TGroup tg = tgroups[gi];
+      const Group G = groups[tg.grp];
+      const int np = tg.src_end - tg.src_begin;
+      const int dar = G.d_ar;
+      // ---- stage 1: Y_p[c][r] = sum_k C_h[r, Q_r col k] rho_b[c, k] ----
+      for (int e = threadIdx.x; e < np * dar; e += blockDim.x) {
+        const int p = e / dar, r = e - p * dar;
+        const TSrc src = tsrcs[tg.src_begin + p];
+        T acc[CH];
 #pragma unroll
-    for (int q = 0; q < AQ; ++q) {
-      const int idx = threadIdx.x + 256 * q;
-      const int i = idx % nl, j = idx / nl;
-      if (j < ncols) {
-        T a = acc[q];
-        for (int k = 0; k < nr; ++k) a = fma(rs[i + nl * k], zs[k * 64 + j], a);
-        acc[q] = a;
+        for (int c = 0; c < CH; ++c) acc[c] = T(0);
+        const T *C = x + src.c + r;
+        const T *R = rhoB + src.rho;
+        for (int k = 0; k < src.nr; ++k) {
+          const T ck = C[(int64_t)dar * k];
+          const T *Rk = R + (int64_t)src.ld_rho * k;
+#pragma unroll
+          for (int c = 0; c < CH; ++c)
+            if (c < nq) acc[c] = fma(ck, __ldg(Rk + c), acc[c]);
+        }
+        T *Yp = scratch + (int64_t)p * CH * dar + r;
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+          if (c < nq) Yp[(int64_t)c * dar] = acc[c];
       }
+      for (int e = threadIdx.x; e < np; e += blockDim.x) sidx_s[e] = tsrcs[tg.src_begin + e].sidx;
+      __syncthreads();
+      for (int e = threadIdx.x; e < G.na * np; e += blockDim.x) {
+        const int a = e / np, p = e - a * np;
+        ws[a * MAXS + p] = W[G.w_off + a * G.nsrc + sidx_s[p]];
+      }
+      __syncthreads();
+      // ---- stage 2: warp items = (P_r, <= 8 rows); mix sources, apply rho_a ----
+      for (int it = G.pr_begin + warp; it < G.pr_end; it += PN_WARPS) {
+        const PrWork pw = prwork[it];
+        const int na = pw.a_end - pw.a_begin;
+        T *z = zs + (size_t)warp * (MAXA * 8 * CH);
+#pragma unroll
+        for (int kk = 0; kk < EPL; ++kk) {
+          const int e = lane + 32 * kk;
+          const int r = e % 8, c = e / 8;
+          const bool ok = (r < pw.nr) && (c < nq);
+          T y[MAXS];
+#pragma unroll
+          for (int p = 0; p < MAXS; ++p)
+            y[p] = (ok && p < np) ? scratch[((int64_t)p * CH + c) * dar + pw.row0 + r] : T(0);
+          for (int ai = 0; ai < na; ++ai) {
+            const T *wr = ws + aops[pw.a_begin + ai].wrow * MAXS;
+            T zz = T(0);
+#pragma unroll
+            for (int p = 0; p < MAXS; ++p)
+              if (p < np) zz = fma(wr[p], y[p], zz);
+            z[(ai * 8 + r) * CH + c] = zz;
+          }
+        }
+        __syncwarp();
+        for (int ai = 0; ai < na; ++ai) {
+          const AOp a = aops[pw.a_begin + ai];
+          const T *zr = z + ai * 8 * CH;
+          for (int e = lane; e < a.nl * nq; e += 32) {
+            const int l = e % a.nl, c = e / a.nl;
+            const T *ra = rhoA + a.rho + l;
+            T v = T(0);
+            for (int r = 0; r < pw.nr; ++r) v = fma(__ldg(ra + (int64_t)a.ld * r), zr[r * CH + c], v);
+            atomicAdd(out_s + (a.out_row0 + l) + dal * c, v);
+          }
+        }
+        __syncwarp();
+      }
+      __syncthreads();  // scratch, ws and sidx_s are rewritten by the next group
+    }
+    for (int e = threadIdx.x; e < dal * nq; e += blockDim.x) {
+      const int r = e % dal, c = e / dal;
+      out[t.out + r + (int64_t)dal * c] += out_s[r + dal * c];
     }
     __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < AQ; ++q) {
-    const int idx = threadIdx.x + 256 * q;
-    const int i = idx % nl, j = idx / nl;
-    if (j < ncols) {
-      T *o = out + t.out + i + (int64_t)t.ld * j;
-      *o += acc[q];
-    }
   }
 }
 
@@ -220,65 +239,60 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ky_smem(const nsx_handle *h, size_t es) {
-  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
-}
-static size_t ka_smem(const nsx_handle *h, size_t es) {
-  return KaLayout(es, h->max_anl, h->max_anr, h->max_mix).total;
+static size_t pn_smem(const PnPlan &P, size_t es) { return PnLayout(es, P.max_dal, P.CH).total; }
+
+template <typename T>
+static void upload_pn(nsx_handle *h, const PnPlan &P, PnDevice &D) {
+  D.groups = dev_copy_pod(P.groups);
+  D.tgroups = dev_copy_pod(P.tgroups);
+  D.tsrcs = dev_copy_pod(P.tsrcs);
+  D.prwork = dev_copy_pod(P.prwork);
+  D.aops = dev_copy_pod(P.aops);
+  D.tasks = dev_copy_pod(P.tasks);
+  D.weights = dev_copy<T>(P.weights);
+  int sms = 0;
+  NSX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  D.grid = std::max(1, std::min<int>(sms, (int)P.tasks.size()));
+  size_t slot = (size_t)std::max(P.max_nsrc, 1) * P.CH * std::max(P.max_dar, 1);
+  NSX_CUDA(cudaMalloc(&D.scratch, slot * sizeof(T) * D.grid));
+  NSX_CUDA(cudaMalloc(&D.counter, sizeof(int)));
+  D.smem = pn_smem(P, sizeof(T));
+  if (D.smem > 227 * 1024) fail(NSX_E_ARG, "k_pn shared-memory layout exceeds 227 KB (output block too tall)");
 }
 
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
-  if (h->max_anl > AQ * 256 / 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
+  for (const PnPlan *P : {&h->pn64, &h->pn32}) {
+    for (const Group &g : P->groups)
+      if (g.na > MAXA || g.nsrc > MAXS) fail(NSX_E_ARG, "pn group exceeds the k_pn operator/source limits");
+  }
   d.rhoA = dev_copy<double>(h->A.vals);
   d.rhoB = dev_copy<double>(h->B.vals);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
-  d.w = dev_copy<double>(h->weights);
-  d.ygroups = dev_copy_pod(h->ygroups);
-  d.yblks = dev_copy_pod(h->yblks);
-  d.atiles = dev_copy_pod(h->atiles);
-  d.acontribs = dev_copy_pod(h->acontribs);
-  d.amixes = dev_copy_pod(h->amixes);
   d.ltiles = dev_copy_pod(h->ltiles);
+  upload_pn<double>(h, h->pn64, d.pn64);
   NSX_CUDA(cudaMalloc(&d.xin, h->no_state * sizeof(double)));
   NSX_CUDA(cudaMalloc(&d.xout, h->no_state * sizeof(double)));
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
-  for (size_t es : {sizeof(double), sizeof(float)}) {
-    if (ky_smem(h, es) > 227 * 1024 || ka_smem(h, es) > 227 * 1024)
-      fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_y / k_a");
-  }
-  NSX_CUDA(cudaFuncSetAttribute(k_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 8)));
-  NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 8)));
-  NSX_CUDA(cudaFuncSetAttribute(k_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 4)));
-  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 4)));
+  NSX_CUDA(cudaFuncSetAttribute(k_pn<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.pn64.smem));
 }
 
 void ensure_precision(nsx_handle *h, int precision) {
   auto &d = h->d;
-  size_t ny = std::max<int64_t>(h->y_elems, 1);
-  if (precision == NSX_FP64) {
-    if (!d.y64) {
-      NSX_CUDA(cudaMalloc(&d.y64, ny * sizeof(double)));
-      NSX_CUDA(cudaMemset(d.y64, 0, ny * sizeof(double)));  // unreachable column slabs stay zero
-    }
-  } else if (precision == NSX_FP32) {
-    if (!d.y32) {
-      NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
-      NSX_CUDA(cudaMemset(d.y32, 0, ny * sizeof(float)));
-      d.rhoA32 = dev_copy<float>(h->A.vals);
-      d.rhoB32 = dev_copy<float>(h->B.vals);
-      d.hA32 = dev_copy<float>(h->A.hdense);
-      d.hB32 = dev_copy<float>(h->B.hdense);
-      d.w32 = dev_copy<float>(h->weights);
-      NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
-      NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
-    }
-  } else {
-    fail(NSX_E_ARG, "unknown precision");
-  }
+  if (precision == NSX_FP64) return;
+  if (precision != NSX_FP32) fail(NSX_E_ARG, "unknown precision");
+  if (d.x32) return;
+  d.rhoA32 = dev_copy<float>(h->A.vals);
+  d.rhoB32 = dev_copy<float>(h->B.vals);
+  d.hA32 = dev_copy<float>(h->A.hdense);
+  d.hB32 = dev_copy<float>(h->B.hdense);
+  upload_pn<float>(h, h->pn32, d.pn32);
+  NSX_CUDA(cudaFuncSetAttribute(k_pn<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.pn32.smem));
+  NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
+  NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
 }
 
 // Brackets one stage launch with events when per-stage timing is enabled.
@@ -317,39 +331,39 @@ void flush_stage_events(nsx_handle *h) {
 }
 
 // Algorithmic traffic (each operand read once, each result written once) and
-// flops of one launch of each stage.
+// flops of one launch of each stage.  k_pn keeps its Y operands on chip/L2, so
+// its algorithmic bytes are the input vector, both density sets and the output.
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]) {
   const double es = precision == NSX_FP64 ? 8.0 : 4.0;
   const double n = (double)h->no_state;
   double rhoA = (double)h->A.vals.size(), rhoB = (double)h->B.vals.size();
   double hd = (double)(h->A.hdense.size() + h->B.hdense.size());
-  bytes[0] = es * (2.0 * n + hd);                               // C in, out written, dense H
-  bytes[1] = es * (n + rhoB + (double)h->y_elems);              // C in, rho_B, Y written
-  bytes[2] = es * ((double)h->y_elems + rhoA + 2.0 * n) + 4.0 * (double)h->weights.size();  // Y, rho_A, out r/w
-  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);     // one conversion launch
+  const PnPlan &P = precision == NSX_FP64 ? h->pn64 : h->pn32;
+  bytes[0] = es * (2.0 * n + hd);
+  bytes[1] = es * (3.0 * n + rhoA + rhoB + (double)P.weights.size());
+  bytes[2] = 0.0;
+  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);
   flops[0] = h->flops_like;
-  flops[1] = h->flops_y;
-  flops[2] = h->flops_mix + h->flops_a;
+  flops[1] = h->flops_y + h->flops_mix + h->flops_a;
+  flops[2] = 0.0;
   flops[3] = 0.0;
 }
 
-template <typename T>
+template <typename T, int CH>
 static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T *rhoB, const T *hA, const T *hB,
-                       const T *w, T *Y, cudaStream_t s) {
+                       const PnPlan &P, const PnDevice &D, cudaStream_t s) {
   auto &d = h->d;
   if (!h->ltiles.empty()) {
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
   }
-  if (!h->ygroups.empty()) {
+  if (!P.tasks.empty()) {
+    NSX_CUDA(cudaMemsetAsync(D.counter, 0, sizeof(int), s));
+    size_t slot = (size_t)std::max(P.max_nsrc, 1) * P.CH * std::max(P.max_dar, 1);
     StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
-                                                                             h->max_ynr, h->max_ynl);
-  }
-  if (!h->atiles.empty()) {
-    StageScope sc(h, 2, s);
-    k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(
-        d.atiles, d.acontribs, d.amixes, w, rhoA, Y, out, h->max_anr, h->max_anl, h->max_mix);
+    k_pn<T, CH><<<D.grid, 512, D.smem, s>>>(D.tasks, (int)P.tasks.size(), D.tgroups, D.groups, D.tsrcs, D.prwork,
+                                            D.aops, (const T *)D.weights, x, rhoA, rhoB, out, (T *)D.scratch,
+                                            (int64_t)slot, D.counter, P.max_dal);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -360,7 +374,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   h->matvecs++;
   h->last_precision = precision;
   if (precision == NSX_FP64) {
-    run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.y64, s);
+    run_stages<double, 8>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, h->pn64, d.pn64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -368,7 +382,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       StageScope sc(h, 3, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.y32, s);
+    run_stages<float, 16>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, h->pn32, d.pn32, s);
     {
       StageScope sc(h, 3, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
@@ -377,12 +391,21 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   }
 }
 
-void release(nsx_handle *h) {
-  auto &d = h->d;
-  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.ygroups, d.yblks,
-                  d.atiles, d.acontribs, d.amixes, d.ltiles, d.y64, d.y32, d.x32, d.o32, d.xin, d.xout};
+static void free_pn(PnDevice &D) {
+  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.prwork, D.aops, D.tasks, D.weights, D.scratch, D.counter};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  D = PnDevice();
+}
+
+void release(nsx_handle *h) {
+  auto &d = h->d;
+  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.ltiles,
+                  d.x32, d.o32, d.xin, d.xout};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  free_pn(d.pn64);
+  free_pn(d.pn32);
   d = DeviceBuffers();
   for (auto &e : h->stage_events) {
     cudaEventDestroy(e.second.first);

@@ -19,7 +19,12 @@ def main():
     for _ in range(reps):
         S.matvec(x.data_ptr(), y.data_ptr(), prec)
     torch.cuda.synchronize()
-    print(name, "dim", S.dim, "ok", float(y.abs().max()))
+    S.stats_reset(timing=True)
+    for _ in range(reps):
+        S.matvec(x.data_ptr(), y.data_ptr(), prec)
+    st = S.stats()["stages"]
+    per = {k: round(v["ms"] / v["launches"], 4) for k, v in st.items() if v["launches"]}
+    print(name, "dim", S.dim, "ok", float(y.abs().max()), "ms/launch", per)
     S.close()
 
 
