@@ -90,36 +90,43 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 
 // ---------------------------------------------------------------------------
 // k_pn: see the file comment.  512 threads (16 warps), one CTA per SM.
+//   scratch slot layout: Y[p][r][c] (p present source, r < d_ar, c < CH)
+//   stage-2 lane map: column c = lane % CH, row sub-index lane / CH
 constexpr int PN_WARPS = 16;
 struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte aligned)
-  size_t out, z, w, sidx, total;
+  size_t out, z, w, src, total;
   __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
+  __host__ __device__ static int ldo(int dal) { return dal | 1; }  // odd: conflict-free column stride
   __host__ __device__ PnLayout(size_t es, int max_dal, int ch) {
     out = 0;
-    z = al(out + es * (size_t)max_dal * ch);
-    w = al(z + es * (size_t)PN_WARPS * MAXA * 8 * ch);
-    sidx = al(w + es * (size_t)MAXA * MAXS);
-    total = al(sidx + 4 * (size_t)MAXS);
+    z = al(out + es * (size_t)ldo(max_dal) * ch);
+    w = al(z + es * (size_t)PN_WARPS * MAXA * ITEM_ROWS * ch);
+    src = al(w + es * (size_t)MAXA * MAXS);
+    total = al(src + sizeof(int) * 2 * (size_t)MAXS);
   }
 };
 
 template <typename T, int CH>
 __global__ void __launch_bounds__(512, 1)
     k_pn(const PnTask *__restrict__ tasks, int ntasks, const TGroup *__restrict__ tgroups,
-         const Group *__restrict__ groups, const TSrc *__restrict__ tsrcs, const PrWork *__restrict__ prwork,
-         const AOp *__restrict__ aops, const T *__restrict__ W, const T *__restrict__ x,
-         const T *__restrict__ rhoA, const T *__restrict__ rhoB, T *__restrict__ out, T *__restrict__ scratch_all,
-         int64_t slot_elems, int *__restrict__ counter, int max_dal) {
-  constexpr int EPL = (8 * CH) / 32;  // stage-2 elements per lane (8 rows x CH columns)
+         const Group *__restrict__ groups, const TSrc *__restrict__ tsrcs, const Piece *__restrict__ pieces,
+         const PrWork *__restrict__ prwork, const AOp *__restrict__ aops, const T *__restrict__ W,
+         const T *__restrict__ x, const T *__restrict__ rhoA, const T *__restrict__ rhoB, T *__restrict__ out,
+         T *__restrict__ scratch_all, int64_t slot_elems, int *__restrict__ counter, int max_dal) {
+  constexpr int LR = 32 / CH;              // lanes per column
+  constexpr int RPL = ITEM_ROWS / LR;      // rows per lane in stage 2
+  static_assert(LR * CH == 32 && RPL * LR == ITEM_ROWS, "lane map");
   extern __shared__ __align__(16) unsigned char smem[];
   const PnLayout L(sizeof(T), max_dal, CH);
-  T *out_s = reinterpret_cast<T *>(smem + L.out);   // [max_dal][CH] column-major (ld = d_al)
-  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][8][CH]
-  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] compact weights
-  int *sidx_s = reinterpret_cast<int *>(smem + L.sidx);
+  T *out_s = reinterpret_cast<T *>(smem + L.out);   // [CH][ldo] : out_s[row + ldo*c]
+  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][ITEM_ROWS][CH]
+  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] weights of the present sources
+  int *sidx_s = reinterpret_cast<int *>(smem + L.src);   // [MAXS]
+  uint32_t *cov_s = reinterpret_cast<uint32_t *>(sidx_s + MAXS);  // [MAXS]
   __shared__ int s_task;
   T *scratch = scratch_all + (int64_t)blockIdx.x * slot_elems;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int lc = lane % CH, lrow = lane / CH;
   for (;;) {
     if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
@@ -127,83 +134,96 @@ __global__ void __launch_bounds__(512, 1)
     __syncthreads();
     if (ti >= ntasks) break;
     const PnTask t = tasks[ti];
-    const int dal = t.d_al, nq = t.nq;
-    for (int e = threadIdx.x; e < dal * CH; e += blockDim.x) out_s[e] = T(0);
+    const int dal = t.d_al, nq = t.nq, ldo = PnLayout::ldo(dal);
+    for (int e = threadIdx.x; e < ldo * CH; e += blockDim.x) out_s[e] = T(0);
     for (int gi = t.g_begin; gi < t.g_end; ++gi) {
       const TGroup tg = tgroups[gi];
       const Group G = groups[tg.grp];
       const int np = tg.src_end - tg.src_begin;
       const int dar = G.d_ar;
-      // ---- stage 1: Y_p[c][r] = sum_k C_h[r, Q_r col k] rho_b[c, k] ----
+      // ---- stage 1: Y_p[r][c] over the pieces of each present source ----
       for (int e = threadIdx.x; e < np * dar; e += blockDim.x) {
         const int p = e / dar, r = e - p * dar;
         const TSrc src = tsrcs[tg.src_begin + p];
-        T acc[CH];
+        T *Yr = scratch + ((int64_t)p * dar + r) * CH;
+        for (int pi = src.piece_begin; pi < src.piece_end; ++pi) {
+          const Piece pc = pieces[pi];
+          const T *C = x + pc.c + r;
+          for (int j0 = 0; j0 < pc.w; j0 += 4) {
+            T acc[4] = {T(0), T(0), T(0), T(0)};
+            const T *R = rhoB + pc.rho + j0;
+            for (int k = 0; k < pc.nr; ++k) {
+              const T ck = C[(int64_t)dar * k];
+              const T *Rk = R + (int64_t)pc.ld * k;
 #pragma unroll
-        for (int c = 0; c < CH; ++c) acc[c] = T(0);
-        const T *C = x + src.c + r;
-        const T *R = rhoB + src.rho;
-        for (int k = 0; k < src.nr; ++k) {
-          const T ck = C[(int64_t)dar * k];
-          const T *Rk = R + (int64_t)src.ld_rho * k;
+              for (int q = 0; q < 4; ++q)
+                if (j0 + q < pc.w) acc[q] = fma(ck, __ldg(Rk + q), acc[q]);
+            }
 #pragma unroll
-          for (int c = 0; c < CH; ++c)
-            if (c < nq) acc[c] = fma(ck, __ldg(Rk + c), acc[c]);
+            for (int q = 0; q < 4; ++q)
+              if (j0 + q < pc.w) Yr[pc.cs + j0 + q] = acc[q];
+          }
         }
-        T *Yp = scratch + (int64_t)p * CH * dar + r;
-#pragma unroll
-        for (int c = 0; c < CH; ++c)
-          if (c < nq) Yp[(int64_t)c * dar] = acc[c];
       }
-      for (int e = threadIdx.x; e < np; e += blockDim.x) sidx_s[e] = tsrcs[tg.src_begin + e].sidx;
+      for (int e = threadIdx.x; e < np; e += blockDim.x) {
+        const TSrc src = tsrcs[tg.src_begin + e];
+        sidx_s[e] = src.sidx;
+        cov_s[e] = src.cover;
+      }
       __syncthreads();
       for (int e = threadIdx.x; e < G.na * np; e += blockDim.x) {
         const int a = e / np, p = e - a * np;
         ws[a * MAXS + p] = W[G.w_off + a * G.nsrc + sidx_s[p]];
       }
       __syncthreads();
-      // ---- stage 2: warp items = (P_r, <= 8 rows); mix sources, apply rho_a ----
+      // ---- stage 2: warp items (P_r, <= ITEM_ROWS rows): mix in registers, apply rho_a ----
       for (int it = G.pr_begin + warp; it < G.pr_end; it += PN_WARPS) {
         const PrWork pw = prwork[it];
         const int na = pw.a_end - pw.a_begin;
-        T *z = zs + (size_t)warp * (MAXA * 8 * CH);
+        T *z = zs + (size_t)warp * (MAXA * ITEM_ROWS * CH);
+        int wrow[MAXA];
 #pragma unroll
-        for (int kk = 0; kk < EPL; ++kk) {
-          const int e = lane + 32 * kk;
-          const int r = e % 8, c = e / 8;
-          const bool ok = (r < pw.nr) && (c < nq);
-          T y[MAXS];
+        for (int ai = 0; ai < MAXA; ++ai) wrow[ai] = ai < na ? aops[pw.a_begin + ai].wrow : 0;
 #pragma unroll
-          for (int p = 0; p < MAXS; ++p)
-            y[p] = (ok && p < np) ? scratch[((int64_t)p * CH + c) * dar + pw.row0 + r] : T(0);
-          for (int ai = 0; ai < na; ++ai) {
-            const T *wr = ws + aops[pw.a_begin + ai].wrow * MAXS;
-            T zz = T(0);
+        for (int rr = 0; rr < RPL; ++rr) {
+          const int r = lrow + LR * rr;
+          const bool ok = r < pw.nr;
+          T zz[MAXA];
 #pragma unroll
-            for (int p = 0; p < MAXS; ++p)
-              if (p < np) zz = fma(wr[p], y[p], zz);
-            z[(ai * 8 + r) * CH + c] = zz;
+          for (int ai = 0; ai < MAXA; ++ai) zz[ai] = T(0);
+          if (ok) {
+            const T *Yc = scratch + (int64_t)(pw.row0 + r) * CH + lc;
+            for (int p = 0; p < np; ++p) {
+              const T y = ((cov_s[p] >> lc) & 1u) ? Yc[(int64_t)p * dar * CH] : T(0);
+#pragma unroll
+              for (int ai = 0; ai < MAXA; ++ai)
+                if (ai < na) zz[ai] = fma(ws[wrow[ai] * MAXS + p], y, zz[ai]);
+            }
           }
+#pragma unroll
+          for (int ai = 0; ai < MAXA; ++ai)
+            if (ai < na) z[(ai * ITEM_ROWS + r) * CH + lc] = ok ? zz[ai] : T(0);
         }
         __syncwarp();
         for (int ai = 0; ai < na; ++ai) {
           const AOp a = aops[pw.a_begin + ai];
-          const T *zr = z + ai * 8 * CH;
-          for (int e = lane; e < a.nl * nq; e += 32) {
-            const int l = e % a.nl, c = e / a.nl;
-            const T *ra = rhoA + a.rho + l;
-            T v = T(0);
-            for (int r = 0; r < pw.nr; ++r) v = fma(__ldg(ra + (int64_t)a.ld * r), zr[r * CH + c], v);
-            atomicAdd(out_s + (a.out_row0 + l) + dal * c, v);
+          const T *zr = z + ai * ITEM_ROWS * CH + lc;
+          if (lc < nq) {
+            for (int l = lrow; l < a.nl; l += LR) {
+              const T *ra = rhoA + a.rho + l;
+              T v = T(0);
+              for (int r = 0; r < pw.nr; ++r) v = fma(__ldg(ra + (int64_t)a.ld * r), zr[r * CH], v);
+              atomicAdd(out_s + (a.out_row0 + l) + ldo * lc, v);
+            }
           }
         }
         __syncwarp();
       }
-      __syncthreads();  // scratch, ws and sidx_s are rewritten by the next group
+      __syncthreads();  // scratch, ws, sidx_s, cov_s are rewritten by the next group
     }
     for (int e = threadIdx.x; e < dal * nq; e += blockDim.x) {
       const int r = e % dal, c = e / dal;
-      out[t.out + r + (int64_t)dal * c] += out_s[r + dal * c];
+      out[t.out + r + (int64_t)dal * c] += out_s[r + ldo * c];
     }
     __syncthreads();
   }
@@ -246,6 +266,7 @@ static void upload_pn(nsx_handle *h, const PnPlan &P, PnDevice &D) {
   D.groups = dev_copy_pod(P.groups);
   D.tgroups = dev_copy_pod(P.tgroups);
   D.tsrcs = dev_copy_pod(P.tsrcs);
+  D.pieces = dev_copy_pod(P.pieces);
   D.prwork = dev_copy_pod(P.prwork);
   D.aops = dev_copy_pod(P.aops);
   D.tasks = dev_copy_pod(P.tasks);
@@ -361,9 +382,9 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
     NSX_CUDA(cudaMemsetAsync(D.counter, 0, sizeof(int), s));
     size_t slot = (size_t)std::max(P.max_nsrc, 1) * P.CH * std::max(P.max_dar, 1);
     StageScope sc(h, 1, s);
-    k_pn<T, CH><<<D.grid, 512, D.smem, s>>>(D.tasks, (int)P.tasks.size(), D.tgroups, D.groups, D.tsrcs, D.prwork,
-                                            D.aops, (const T *)D.weights, x, rhoA, rhoB, out, (T *)D.scratch,
-                                            (int64_t)slot, D.counter, P.max_dal);
+    k_pn<T, CH><<<D.grid, 512, D.smem, s>>>(D.tasks, (int)P.tasks.size(), D.tgroups, D.groups, D.tsrcs, D.pieces,
+                                            D.prwork, D.aops, (const T *)D.weights, x, rhoA, rhoB, out,
+                                            (T *)D.scratch, (int64_t)slot, D.counter, P.max_dal);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -392,7 +413,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
 }
 
 static void free_pn(PnDevice &D) {
-  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.prwork, D.aops, D.tasks, D.weights, D.scratch, D.counter};
+  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.pieces, D.prwork, D.aops, D.tasks, D.weights, D.scratch, D.counter};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   D = PnDevice();

@@ -66,6 +66,7 @@ struct TabRow {     // one (output block, J_ar, proton density key)
 // ---- plan of the fused pn kernel k_pn ---------------------------------------------
 constexpr int MAXA = 16;    // proton operators per work item
 constexpr int MAXS = 32;    // sources (h, b) per group
+constexpr int ITEM_ROWS = 4; // proton rows per stage-2 work item
 struct Group {              // (output block, J_ar, lam): shared by the block's tasks
   int32_t d_ar;             // proton rows of the Y operands (d_a(J_ar))
   int32_t nsrc;             // sources of the group (<= MAXS)
@@ -77,15 +78,19 @@ struct TGroup {             // a group as seen by one task: the sources present 
   int32_t grp;
   int32_t src_begin, src_end;
 };
-struct TSrc {               // Y_s[:, chunk] = C_h[:, Q_r cols] rho_b[chunk rows, Q_r]^T
-  int64_t c;                // offset of C_h[0, first column of Q_r]
-  int64_t rho;              // offset of rho_b(Q_l, Q_r) element (chunk row 0, col 0)
-  int32_t ld_rho;           // n(Q_l): leading dimension of that block
-  int32_t nr;               // n(Q_r)
+struct TSrc {               // a group source present in a task's column chunk
+  int32_t piece_begin, piece_end;  // range in pieces
+  uint32_t cover;           // chunk columns the pieces cover (bit c)
   int32_t sidx;             // source index within the group
-  int32_t pad;
 };
-struct PrWork {             // <= 8 rows of one proton right partition P_r
+struct Piece {              // Y_s[:, cs..cs+w) = C_h[:, Q_r cols] rho_b[rows.., Q_r]^T
+  int64_t c;                // offset of C_h[0, first column of Q_r]
+  int64_t rho;              // offset of rho_b(Q_l, Q_r) element (first row of the piece, col 0)
+  int32_t ld;               // n(Q_l): leading dimension of the density block
+  int32_t nr;               // n(Q_r)
+  int32_t cs, w;            // chunk columns [cs, cs+w)
+};
+struct PrWork {             // <= 4 rows of one proton right partition P_r
   int32_t row0, nr;
   int32_t a_begin, a_end;   // range in aops (<= MAXA)
 };
@@ -93,7 +98,7 @@ struct AOp {                // proton density block rho_a(P_l, P_r), rows chunk 
   int64_t rho;              // offset of element (0, chunk row 0); block nl x n(P_r) column-major
   int32_t ld, out_row0, nl, wrow;
 };
-struct PnTask {             // output block, neutron partition Q_l, <= CH of its states
+struct PnTask {             // output block, CH consecutive neutron states (columns)
   int64_t out;              // offset of out[row 0, first column]
   int32_t d_al, nq;
   int32_t g_begin, g_end;   // range in tgroups
@@ -103,6 +108,7 @@ struct PnPlan {
   std::vector<Group> groups;
   std::vector<TGroup> tgroups;
   std::vector<TSrc> tsrcs;
+  std::vector<Piece> pieces;
   std::vector<PrWork> prwork;
   std::vector<AOp> aops;
   std::vector<PnTask> tasks;
@@ -114,6 +120,7 @@ struct PnDevice {           // device copy of one plan (typed operand data lives
   Group *groups = nullptr;
   TGroup *tgroups = nullptr;
   TSrc *tsrcs = nullptr;
+  Piece *pieces = nullptr;
   PrWork *prwork = nullptr;
   AOp *aops = nullptr;
   PnTask *tasks = nullptr;

@@ -2,8 +2,8 @@
 // reference's drdbh (src/NuLnz/NuCoreX.f90:1428-1577), regrouped for a GPU
 // that owns output columns.
 //
-// Output block (Ja_l, Jb_l) is cut into tasks = (neutron partition Q_l, chunk of
-// at most CH of its states).  Everything a task needs is local to it:
+// Output block (Ja_l, Jb_l) is cut into tasks = CH consecutive neutron states
+// (output columns, possibly spanning several partitions Q_l).  Everything a task needs is local to it:
 //   Y_(h,b)[:, chunk] = C_h[:, Q_r(b) cols] rho_b[chunk, Q_r]^T    (Y columns are output columns)
 //   Z_a[P_r rows]     = sum_(h,b) w_(a,(h,b)) Y_(h,b)[P_r rows]    (mixing)
 //   out[P_l rows]    += rho_a[P_l, P_r] Z_a[P_r rows]
@@ -87,9 +87,6 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
   // groups per output block: (J_ar, lam) -> table rows
   std::map<int, std::map<std::pair<int, int>, std::vector<int>>> by_block;
   for (size_t i = 0; i < table.size(); ++i) by_block[table[i].bl][{table[i].jar, table[i].lam}].push_back((int)i);
-  struct GroupSrc {
-    std::vector<std::pair<int, int>> src;  // (h block, b key)
-  };
   for (auto &bk : by_block) {
     const int bl = bk.first;
     const Block &ob = h->blocks[bl];
@@ -124,7 +121,7 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
           }
           P.weights.insert(P.weights.end(), wr.begin(), wr.end());
         }
-        // right proton partitions: operators acting on each, rows in chunks of 8
+        // right proton partitions: operators acting on each, rows in chunks of ITEM_ROWS
         G.pr_begin = (int)P.prwork.size();
         for (int pr = 0; pr < A.nspart; ++pr) {
           int nr = A.njt_of(pr, jar);
@@ -134,11 +131,11 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
             for (const RhoBlk &rb : A.kblocks[table[rows[ai]].ak])
               if (rb.pr == pr) ops.push_back({(int)ai, &rb});
           if (ops.empty()) continue;
-          for (int r0 = 0; r0 < nr; r0 += 8) {
+          for (int r0 = 0; r0 < nr; r0 += ITEM_ROWS) {
             for (size_t o0 = 0; o0 < ops.size(); o0 += MAXA) {
               PrWork w;
               w.row0 = A.poff[A.jidx(jar)][pr] + r0;
-              w.nr = std::min(8, nr - r0);
+              w.nr = std::min(ITEM_ROWS, nr - r0);
               w.a_begin = (int)P.aops.size();
               for (size_t o = o0; o < std::min(ops.size(), o0 + MAXA); ++o) {
                 const RhoBlk *rb = ops[o].second;
@@ -165,47 +162,59 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
         P.max_nsrc = std::max(P.max_nsrc, G.nsrc);
       }
     }
-    // tasks: neutron left partition Q_l, chunks of CH states
-    for (int ql = 0; ql < B.nspart; ++ql) {
-      int nql = B.njt_of(ql, ob.J2b);
-      if (nql == 0) continue;
-      for (int c0 = 0; c0 < nql; c0 += CH) {
-        PnTask t;
-        t.out = ob.off + (int64_t)(B.poff[B.jidx(ob.J2b)][ql] + c0) * ob.da;
-        t.d_al = ob.da;
-        t.nq = std::min(CH, nql - c0);
-        t.g_begin = (int)P.tgroups.size();
-        double cost = 0;
-        for (size_t gi = 0; gi < gids.size(); ++gi) {
-          const Group &G = P.groups[gids[gi]];
-          TGroup tg;
-          tg.grp = gids[gi];
-          tg.src_begin = (int)P.tsrcs.size();
-          for (int s = 0; s < (int)gsrc[gi].size(); ++s) {
-            int hb = gsrc[gi][s].first, bkey = gsrc[gi][s].second;
+    // tasks: CH consecutive neutron states (columns) of the output block
+    const int jbl = B.jidx(ob.J2b);
+    for (int c0 = 0; c0 < ob.db; c0 += CH) {
+      PnTask t;
+      t.out = ob.off + (int64_t)c0 * ob.da;
+      t.d_al = ob.da;
+      t.nq = std::min(CH, ob.db - c0);
+      t.g_begin = (int)P.tgroups.size();
+      double cost = 0;
+      for (size_t gi = 0; gi < gids.size(); ++gi) {
+        const Group &G = P.groups[gids[gi]];
+        TGroup tg;
+        tg.grp = gids[gi];
+        tg.src_begin = (int)P.tsrcs.size();
+        for (int s = 0; s < (int)gsrc[gi].size(); ++s) {
+          int hb = gsrc[gi][s].first, bkey = gsrc[gi][s].second;
+          int J2br = h->blocks[hb].J2b;
+          TSrc ts;
+          ts.piece_begin = (int)P.pieces.size();
+          ts.cover = 0u;
+          ts.sidx = s;
+          // left partitions overlapping [c0, c0 + nq)
+          for (int ql = 0; ql < B.nspart; ++ql) {
+            int q0 = B.poff[jbl][ql], q1 = B.poff[jbl][ql + 1];
+            int a0 = std::max(q0, c0), a1 = std::min(q1, c0 + t.nq);
+            if (a0 >= a1) continue;
             auto lk = bl_lookup[bkey][ql];
             if (lk.first < 0) continue;
-            int J2br = h->blocks[hb].J2b;
-            TSrc ts;
-            ts.c = h->blocks[hb].off + (int64_t)B.poff[B.jidx(J2br)][lk.first] * G.d_ar;
-            ts.rho = lk.second + c0;
-            ts.ld_rho = nql;
-            ts.nr = B.njt_of(lk.first, J2br);
-            ts.sidx = s;
-            P.tsrcs.push_back(ts);
-            cost += (double)G.d_ar * t.nq * ts.nr;
+            Piece pc;
+            pc.c = h->blocks[hb].off + (int64_t)B.poff[B.jidx(J2br)][lk.first] * G.d_ar;
+            pc.rho = lk.second + (a0 - q0);
+            pc.ld = q1 - q0;
+            pc.nr = B.njt_of(lk.first, J2br);
+            pc.cs = a0 - c0;
+            pc.w = a1 - a0;
+            for (int c = pc.cs; c < pc.cs + pc.w; ++c) ts.cover |= (1u << c);
+            P.pieces.push_back(pc);
+            cost += (double)G.d_ar * pc.w * pc.nr;
           }
-          tg.src_end = (int)P.tsrcs.size();
-          if (tg.src_end == tg.src_begin) continue;
-          cost += (double)(G.pr_end - G.pr_begin) * 8 * t.nq * (tg.src_end - tg.src_begin);
-          P.tgroups.push_back(tg);
+          ts.piece_end = (int)P.pieces.size();
+          if (ts.piece_end == ts.piece_begin) continue;
+          P.tsrcs.push_back(ts);
         }
-        t.g_end = (int)P.tgroups.size();
-        if (t.g_end == t.g_begin) continue;
-        P.tasks.push_back(t);
-        P.task_cost.push_back(cost);
-        P.max_dal = std::max(P.max_dal, ob.da);
+        tg.src_end = (int)P.tsrcs.size();
+        if (tg.src_end == tg.src_begin) continue;
+        cost += (double)(G.pr_end - G.pr_begin) * ITEM_ROWS * CH * (tg.src_end - tg.src_begin);
+        P.tgroups.push_back(tg);
       }
+      t.g_end = (int)P.tgroups.size();
+      if (t.g_end == t.g_begin) continue;
+      P.tasks.push_back(t);
+      P.task_cost.push_back(cost);
+      P.max_dal = std::max(P.max_dal, ob.da);
     }
   }
   // longest tasks first (greedy balance over the persistent CTAs)

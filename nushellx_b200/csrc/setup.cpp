@@ -226,8 +226,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       h->flops_mix += 2.0 * nr * ob.db * r.e.size();
     }
   }
-  build_pn_plan(h, table, 8, h->pn64);
-  build_pn_plan(h, table, 16, h->pn32);
+  build_pn_plan(h, table, 8, h->pn64);   // FP64: 8 columns per task
+  build_pn_plan(h, table, 16, h->pn32);  // FP32: 16 columns per task
 }
 
 double racah_weight_ext(int Jal, int Jbl, int Jar, int Jbr, int J, int lam) {
