@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 // ---------------------------------------------------------------------------
 // k_pn: see the file comment.  512 threads (16 warps), one CTA per SM.
 //   scratch slot layout: Y[p][r][c] (p present source, r < d_ar, c < CH)
-//   stage-2 lane map: column c = lane % CH, row sub-index lane / CH
+//   stage-2 lane map: column c = lane % CH, row lane / CH (32 / CH rows per item)
 constexpr int PN_WARPS = 16;
 struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte aligned)
   size_t out, z, w, src, total;
@@ -100,11 +100,29 @@ struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte ali
   __host__ __device__ PnLayout(size_t es, int max_dal, int ch) {
     out = 0;
     z = al(out + es * (size_t)ldo(max_dal) * ch);
-    w = al(z + es * (size_t)PN_WARPS * MAXA * ITEM_ROWS * ch);
+    w = al(z + es * (size_t)PN_WARPS * MAXA * (32 / ch) * ch);
     src = al(w + es * (size_t)MAXA * MAXS);
     total = al(src + sizeof(int) * 2 * (size_t)MAXS);
   }
 };
+
+// Stage-2 mixing of one lane's element: z_a = sum_p W[a][p] y_p for the item's
+// operators, y_p loaded once into registers (NP = 16 or 32 sources, zero-padded).
+template <typename T, int NP, int CH>
+__device__ __forceinline__ void pn_mix(const T *__restrict__ Yc, int64_t pstride, int np, const uint32_t *cov,
+                                       int lc, bool ok, const T *ws, const AOp *__restrict__ aops, int a_begin,
+                                       int na, T *zrow) {
+  T y[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) y[p] = (ok && p < np && ((cov[p] >> lc) & 1u)) ? Yc[p * pstride] : T(0);
+  for (int ai = 0; ai < na; ++ai) {
+    const T *wr = ws + __ldg(&aops[a_begin + ai].wrow) * MAXS;
+    T zz = T(0);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) zz = fma(wr[p], y[p], zz);
+    zrow[ai * 32] = zz;
+  }
+}
 
 template <typename T, int CH>
 __global__ void __launch_bounds__(512, 1)
@@ -113,14 +131,12 @@ __global__ void __launch_bounds__(512, 1)
          const PrWork *__restrict__ prwork, const AOp *__restrict__ aops, const T *__restrict__ W,
          const T *__restrict__ x, const T *__restrict__ rhoA, const T *__restrict__ rhoB, T *__restrict__ out,
          T *__restrict__ scratch_all, int64_t slot_elems, int *__restrict__ counter, int max_dal) {
-  constexpr int LR = 32 / CH;              // lanes per column
-  constexpr int RPL = ITEM_ROWS / LR;      // rows per lane in stage 2
-  static_assert(LR * CH == 32 && RPL * LR == ITEM_ROWS, "lane map");
+  constexpr int IR = 32 / CH;              // rows per work item: one (row, column) element per lane
   extern __shared__ __align__(16) unsigned char smem[];
   const PnLayout L(sizeof(T), max_dal, CH);
   T *out_s = reinterpret_cast<T *>(smem + L.out);   // [CH][ldo] : out_s[row + ldo*c]
-  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][ITEM_ROWS][CH]
-  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] weights of the present sources
+  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][32 lanes]
+  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] weights of the present sources (0-padded)
   int *sidx_s = reinterpret_cast<int *>(smem + L.src);   // [MAXS]
   uint32_t *cov_s = reinterpret_cast<uint32_t *>(sidx_s + MAXS);  // [MAXS]
   __shared__ int s_task;
@@ -165,51 +181,40 @@ __global__ void __launch_bounds__(512, 1)
           }
         }
       }
-      for (int e = threadIdx.x; e < np; e += blockDim.x) {
-        const TSrc src = tsrcs[tg.src_begin + e];
-        sidx_s[e] = src.sidx;
-        cov_s[e] = src.cover;
+      for (int e = threadIdx.x; e < MAXS; e += blockDim.x) {
+        if (e < np) {
+          const TSrc src = tsrcs[tg.src_begin + e];
+          sidx_s[e] = src.sidx;
+          cov_s[e] = src.cover;
+        } else {
+          sidx_s[e] = 0;
+          cov_s[e] = 0u;
+        }
       }
       __syncthreads();
-      for (int e = threadIdx.x; e < G.na * np; e += blockDim.x) {
-        const int a = e / np, p = e - a * np;
-        ws[a * MAXS + p] = W[G.w_off + a * G.nsrc + sidx_s[p]];
+      for (int e = threadIdx.x; e < G.na * MAXS; e += blockDim.x) {
+        const int a = e / MAXS, p = e - a * MAXS;
+        ws[e] = p < np ? W[G.w_off + a * G.nsrc + sidx_s[p]] : T(0);
       }
       __syncthreads();
-      // ---- stage 2: warp items (P_r, <= ITEM_ROWS rows): mix in registers, apply rho_a ----
+      // ---- stage 2: warp items (P_r, <= IR rows); lane = (row lrow, column lc) ----
       for (int it = G.pr_begin + warp; it < G.pr_end; it += PN_WARPS) {
         const PrWork pw = prwork[it];
         const int na = pw.a_end - pw.a_begin;
-        T *z = zs + (size_t)warp * (MAXA * ITEM_ROWS * CH);
-        int wrow[MAXA];
-#pragma unroll
-        for (int ai = 0; ai < MAXA; ++ai) wrow[ai] = ai < na ? aops[pw.a_begin + ai].wrow : 0;
-#pragma unroll
-        for (int rr = 0; rr < RPL; ++rr) {
-          const int r = lrow + LR * rr;
-          const bool ok = r < pw.nr;
-          T zz[MAXA];
-#pragma unroll
-          for (int ai = 0; ai < MAXA; ++ai) zz[ai] = T(0);
-          if (ok) {
-            const T *Yc = scratch + (int64_t)(pw.row0 + r) * CH + lc;
-            for (int p = 0; p < np; ++p) {
-              const T y = ((cov_s[p] >> lc) & 1u) ? Yc[(int64_t)p * dar * CH] : T(0);
-#pragma unroll
-              for (int ai = 0; ai < MAXA; ++ai)
-                if (ai < na) zz[ai] = fma(ws[wrow[ai] * MAXS + p], y, zz[ai]);
-            }
-          }
-#pragma unroll
-          for (int ai = 0; ai < MAXA; ++ai)
-            if (ai < na) z[(ai * ITEM_ROWS + r) * CH + lc] = ok ? zz[ai] : T(0);
-        }
+        T *z = zs + (size_t)warp * (MAXA * 32);
+        const bool ok = lrow < pw.nr;
+        const T *Yc = scratch + (int64_t)(pw.row0 + lrow) * CH + lc;
+        const int64_t pstride = (int64_t)dar * CH;
+        if (np <= 16)
+          pn_mix<T, 16, CH>(Yc, pstride, np, cov_s, lc, ok, ws, aops, pw.a_begin, na, z + lane);
+        else
+          pn_mix<T, 32, CH>(Yc, pstride, np, cov_s, lc, ok, ws, aops, pw.a_begin, na, z + lane);
         __syncwarp();
         for (int ai = 0; ai < na; ++ai) {
           const AOp a = aops[pw.a_begin + ai];
-          const T *zr = z + ai * ITEM_ROWS * CH + lc;
+          const T *zr = z + ai * 32 + lc;   // z of (row r, column lc) sits at lane r*CH + lc
           if (lc < nq) {
-            for (int l = lrow; l < a.nl; l += LR) {
+            for (int l = lrow; l < a.nl; l += IR) {
               const T *ra = rhoA + a.rho + l;
               T v = T(0);
               for (int r = 0; r < pw.nr; ++r) v = fma(__ldg(ra + (int64_t)a.ld * r), zr[r * CH], v);

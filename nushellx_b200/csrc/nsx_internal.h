@@ -66,7 +66,6 @@ struct TabRow {     // one (output block, J_ar, proton density key)
 // ---- plan of the fused pn kernel k_pn ---------------------------------------------
 constexpr int MAXA = 16;    // proton operators per work item
 constexpr int MAXS = 32;    // sources (h, b) per group
-constexpr int ITEM_ROWS = 4; // proton rows per stage-2 work item
 struct Group {              // (output block, J_ar, lam): shared by the block's tasks
   int32_t d_ar;             // proton rows of the Y operands (d_a(J_ar))
   int32_t nsrc;             // sources of the group (<= MAXS)
@@ -90,7 +89,7 @@ struct Piece {              // Y_s[:, cs..cs+w) = C_h[:, Q_r cols] rho_b[rows..,
   int32_t nr;               // n(Q_r)
   int32_t cs, w;            // chunk columns [cs, cs+w)
 };
-struct PrWork {             // <= 4 rows of one proton right partition P_r
+struct PrWork {             // <= item_rows rows of one proton right partition P_r
   int32_t row0, nr;
   int32_t a_begin, a_end;   // range in aops (<= MAXA)
 };
@@ -105,6 +104,7 @@ struct PnTask {             // output block, CH consecutive neutron states (colu
 };
 struct PnPlan {
   int CH = 8;
+  int item_rows = 4;        // = 32 / CH: one row per lane in stage 2
   std::vector<Group> groups;
   std::vector<TGroup> tgroups;
   std::vector<TSrc> tsrcs;

@@ -78,6 +78,8 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
   const SpeciesPlan &A = h->A, &B = h->B;
   P = PnPlan();
   P.CH = CH;
+  P.item_rows = 32 / CH;
+  const int IR = P.item_rows;
   // per b-key: left partition -> (right partition, value offset)
   std::vector<std::vector<std::pair<int, int64_t>>> bl_lookup(B.keys.size());
   for (size_t k = 0; k < B.keys.size(); ++k) {
@@ -121,7 +123,7 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
           }
           P.weights.insert(P.weights.end(), wr.begin(), wr.end());
         }
-        // right proton partitions: operators acting on each, rows in chunks of ITEM_ROWS
+        // right proton partitions: operators acting on each, rows in chunks of item_rows
         G.pr_begin = (int)P.prwork.size();
         for (int pr = 0; pr < A.nspart; ++pr) {
           int nr = A.njt_of(pr, jar);
@@ -131,11 +133,11 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
             for (const RhoBlk &rb : A.kblocks[table[rows[ai]].ak])
               if (rb.pr == pr) ops.push_back({(int)ai, &rb});
           if (ops.empty()) continue;
-          for (int r0 = 0; r0 < nr; r0 += ITEM_ROWS) {
+          for (int r0 = 0; r0 < nr; r0 += IR) {
             for (size_t o0 = 0; o0 < ops.size(); o0 += MAXA) {
               PrWork w;
               w.row0 = A.poff[A.jidx(jar)][pr] + r0;
-              w.nr = std::min(ITEM_ROWS, nr - r0);
+              w.nr = std::min(IR, nr - r0);
               w.a_begin = (int)P.aops.size();
               for (size_t o = o0; o < std::min(ops.size(), o0 + MAXA); ++o) {
                 const RhoBlk *rb = ops[o].second;
@@ -207,7 +209,7 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
         }
         tg.src_end = (int)P.tsrcs.size();
         if (tg.src_end == tg.src_begin) continue;
-        cost += (double)(G.pr_end - G.pr_begin) * ITEM_ROWS * CH * (tg.src_end - tg.src_begin);
+        cost += (double)(G.pr_end - G.pr_begin) * IR * CH * (tg.src_end - tg.src_begin);
         P.tgroups.push_back(tg);
       }
       t.g_end = (int)P.tgroups.size();
