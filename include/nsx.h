@@ -160,6 +160,8 @@ typedef struct nsx_stats {
   double stage_ms[4];         /* summed device time per stage (timing enabled only) */
   double stage_bytes[4];      /* algorithmic HBM bytes of one launch of each stage  */
   double stage_flops[4];      /* algorithmic flops of one launch of each stage      */
+  double pn_cycles[4];        /* k_pn SM cycles summed over CTAs (timing enabled):
+                                 Y operands, weights, mixing + proton side, epilogue */
 } nsx_stats;
 
 /* Reset the counters; enable (1) or disable (0) per-stage event timing. */

@@ -10,13 +10,13 @@
 //   k_pn   : persistent; a CTA owns the output columns of one neutron partition
 //            Q_l (a chunk of CH states) of one block and, for every (J_ar, lam)
 //            group of the pn table,
-//              stage 1: Y_(h,b)[:, chunk] = C_h[:, Q_r cols] rho_b[chunk, Q_r]^T
-//                       into the CTA's scratch slot (written and read back by the
-//                       same CTA: it stays in L2, ~0.5 MB per CTA in flight);
-//              stage 2: per proton partition P_r (8 rows per warp item) the
-//                       sources are mixed in registers, Z_a = sum w_(a,s) Y_s,
-//                       and out[P_l rows] += rho_a[P_l, P_r] Z_a is accumulated
-//                       in shared memory.
+//            in batches of at most 64 (FP32) / 32 (FP64) proton rows:
+//              stage 1: Y_(h,b)[batch rows, chunk] = C_h[rows, Q_r cols] rho_b[chunk, Q_r]^T
+//                       straight into shared memory (Y never leaves the SM);
+//              stage 2: per proton partition P_r (32/CH rows per warp item, one
+//                       element per lane) the sources are mixed in registers,
+//                       Z_a = sum w_(a,s) Y_s, and out[P_l rows] += rho_a[P_l, P_r] Z_a
+//                       is accumulated in shared memory.
 //            Each Y_(h,b) element is computed once (the reference recomputes the
 //            neutron-side product for every proton operator).
 //
@@ -90,33 +90,33 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 
 // ---------------------------------------------------------------------------
 // k_pn: see the file comment.  512 threads (16 warps), one CTA per SM.
-//   scratch slot layout: Y[p][r][c] (p present source, r < d_ar, c < CH)
+//   shared Y batch layout: ybuf[p][row - batch row0][c] with odd row stride CH + 1
 //   stage-2 lane map: column c = lane % CH, row lane / CH (32 / CH rows per item)
 constexpr int PN_WARPS = 16;
 struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte aligned)
-  size_t out, z, w, src, total;
+  size_t out, z, w, src, y, total;
   __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
   __host__ __device__ static int ldo(int dal) { return dal | 1; }  // odd: conflict-free column stride
-  __host__ __device__ PnLayout(size_t es, int max_dal, int ch) {
+  __host__ __device__ PnLayout(size_t es, int max_dal, int ch, int batch_rows) {
     out = 0;
     z = al(out + es * (size_t)ldo(max_dal) * ch);
-    w = al(z + es * (size_t)PN_WARPS * MAXA * (32 / ch) * ch);
+    w = al(z + es * (size_t)PN_WARPS * MAXA * 32);
     src = al(w + es * (size_t)MAXA * MAXS);
-    total = al(src + sizeof(int) * 2 * (size_t)MAXS);
+    y = al(src + sizeof(int) * 2 * (size_t)MAXS);
+    total = al(y + es * (size_t)MAXS * batch_rows * (ch + 1));
   }
 };
 
 // Stage-2 mixing of one lane's element: z_a = sum_p W[a][p] y_p for the item's
-// operators, y_p loaded once into registers (NP = 16 or 32 sources, zero-padded).
-template <typename T, int NP, int CH>
-__device__ __forceinline__ void pn_mix(const T *__restrict__ Yc, int64_t pstride, int np, const uint32_t *cov,
-                                       int lc, bool ok, const T *ws, const AOp *__restrict__ aops, int a_begin,
-                                       int na, T *zrow) {
+// operators, y_p read once into registers (NP = 16 or 32 sources, zero-padded).
+template <typename T, int NP>
+__device__ __forceinline__ void pn_mix(const T *Yc, int pstride, int np, const uint32_t *cov, int lc, bool ok,
+                                       const T *ws, int my_wrow, int na, T *zrow) {
   T y[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) y[p] = (ok && p < np && ((cov[p] >> lc) & 1u)) ? Yc[p * pstride] : T(0);
   for (int ai = 0; ai < na; ++ai) {
-    const T *wr = ws + __ldg(&aops[a_begin + ai].wrow) * MAXS;
+    const T *wr = ws + __shfl_sync(0xffffffffu, my_wrow, ai) * MAXS;
     T zz = T(0);
 #pragma unroll
     for (int p = 0; p < NP; ++p) zz = fma(wr[p], y[p], zz);
@@ -128,21 +128,33 @@ template <typename T, int CH>
 __global__ void __launch_bounds__(512, 1)
     k_pn(const PnTask *__restrict__ tasks, int ntasks, const TGroup *__restrict__ tgroups,
          const Group *__restrict__ groups, const TSrc *__restrict__ tsrcs, const Piece *__restrict__ pieces,
-         const PrWork *__restrict__ prwork, const AOp *__restrict__ aops, const T *__restrict__ W,
-         const T *__restrict__ x, const T *__restrict__ rhoA, const T *__restrict__ rhoB, T *__restrict__ out,
-         T *__restrict__ scratch_all, int64_t slot_elems, int *__restrict__ counter, int max_dal) {
+         const PrWork *__restrict__ prwork, const Batch *__restrict__ batches, const AOp *__restrict__ aops,
+         const T *__restrict__ W, const T *__restrict__ x, const T *__restrict__ rhoA, const T *__restrict__ rhoB,
+         T *__restrict__ out, int *__restrict__ counter, int max_dal, int batch_rows,
+         unsigned long long *__restrict__ cycles) {
   constexpr int IR = 32 / CH;              // rows per work item: one (row, column) element per lane
+  constexpr int CHP = CH + 1;              // padded row stride of the Y batch (odd)
   extern __shared__ __align__(16) unsigned char smem[];
-  const PnLayout L(sizeof(T), max_dal, CH);
+  const PnLayout L(sizeof(T), max_dal, CH, batch_rows);
   T *out_s = reinterpret_cast<T *>(smem + L.out);   // [CH][ldo] : out_s[row + ldo*c]
   T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][32 lanes]
   T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] weights of the present sources (0-padded)
-  int *sidx_s = reinterpret_cast<int *>(smem + L.src);   // [MAXS]
+  int *sidx_s = reinterpret_cast<int *>(smem + L.src);            // [MAXS]
   uint32_t *cov_s = reinterpret_cast<uint32_t *>(sidx_s + MAXS);  // [MAXS]
+  T *ybuf = reinterpret_cast<T *>(smem + L.y);      // [p][batch row][CHP]
+  const int pstride = batch_rows * CHP;
   __shared__ int s_task;
-  T *scratch = scratch_all + (int64_t)blockIdx.x * slot_elems;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int lc = lane % CH, lrow = lane / CH;
+  unsigned long long cyc[4] = {0, 0, 0, 0};
+  long long t0 = clock64();
+  auto mark = [&](int k) {
+    if (cycles && threadIdx.x == 0) {
+      long long t1 = clock64();
+      cyc[k] += (unsigned long long)(t1 - t0);
+      t0 = t1;
+    }
+  };
   for (;;) {
     if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
     __syncthreads();
@@ -157,30 +169,6 @@ __global__ void __launch_bounds__(512, 1)
       const Group G = groups[tg.grp];
       const int np = tg.src_end - tg.src_begin;
       const int dar = G.d_ar;
-      // ---- stage 1: Y_p[r][c] over the pieces of each present source ----
-      for (int e = threadIdx.x; e < np * dar; e += blockDim.x) {
-        const int p = e / dar, r = e - p * dar;
-        const TSrc src = tsrcs[tg.src_begin + p];
-        T *Yr = scratch + ((int64_t)p * dar + r) * CH;
-        for (int pi = src.piece_begin; pi < src.piece_end; ++pi) {
-          const Piece pc = pieces[pi];
-          const T *C = x + pc.c + r;
-          for (int j0 = 0; j0 < pc.w; j0 += 4) {
-            T acc[4] = {T(0), T(0), T(0), T(0)};
-            const T *R = rhoB + pc.rho + j0;
-            for (int k = 0; k < pc.nr; ++k) {
-              const T ck = C[(int64_t)dar * k];
-              const T *Rk = R + (int64_t)pc.ld * k;
-#pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (j0 + q < pc.w) acc[q] = fma(ck, __ldg(Rk + q), acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              if (j0 + q < pc.w) Yr[pc.cs + j0 + q] = acc[q];
-          }
-        }
-      }
       for (int e = threadIdx.x; e < MAXS; e += blockDim.x) {
         if (e < np) {
           const TSrc src = tsrcs[tg.src_begin + e];
@@ -196,42 +184,92 @@ __global__ void __launch_bounds__(512, 1)
         const int a = e / MAXS, p = e - a * MAXS;
         ws[e] = p < np ? W[G.w_off + a * G.nsrc + sidx_s[p]] : T(0);
       }
-      __syncthreads();
-      // ---- stage 2: warp items (P_r, <= IR rows); lane = (row lrow, column lc) ----
-      for (int it = G.pr_begin + warp; it < G.pr_end; it += PN_WARPS) {
-        const PrWork pw = prwork[it];
-        const int na = pw.a_end - pw.a_begin;
-        T *z = zs + (size_t)warp * (MAXA * 32);
-        const bool ok = lrow < pw.nr;
-        const T *Yc = scratch + (int64_t)(pw.row0 + lrow) * CH + lc;
-        const int64_t pstride = (int64_t)dar * CH;
-        if (np <= 16)
-          pn_mix<T, 16, CH>(Yc, pstride, np, cov_s, lc, ok, ws, aops, pw.a_begin, na, z + lane);
-        else
-          pn_mix<T, 32, CH>(Yc, pstride, np, cov_s, lc, ok, ws, aops, pw.a_begin, na, z + lane);
-        __syncwarp();
-        for (int ai = 0; ai < na; ++ai) {
-          const AOp a = aops[pw.a_begin + ai];
-          const T *zr = z + ai * 32 + lc;   // z of (row r, column lc) sits at lane r*CH + lc
-          if (lc < nq) {
-            for (int l = lrow; l < a.nl; l += IR) {
-              const T *ra = rhoA + a.rho + l;
-              T v = T(0);
-              for (int r = 0; r < pw.nr; ++r) v = fma(__ldg(ra + (int64_t)a.ld * r), zr[r * CH], v);
-              atomicAdd(out_s + (a.out_row0 + l) + ldo * lc, v);
+      mark(1);
+      for (int bi = G.bt_begin; bi < G.bt_end; ++bi) {
+        const Batch bt = batches[bi];
+        // ---- stage 1: Y_p[row][c] for the batch rows, into shared memory ----
+        for (int e = threadIdx.x; e < np * bt.nrows; e += blockDim.x) {
+          const int p = e / bt.nrows, rr = e - p * bt.nrows;
+          const int r = bt.row0 + rr;
+          const TSrc src = tsrcs[tg.src_begin + p];
+          T *Yr = ybuf + p * pstride + rr * CHP;
+          for (int pi = src.piece_begin; pi < src.piece_end; ++pi) {
+            const Piece pc = pieces[pi];
+            const T *C = x + pc.c + r;
+            for (int j0 = 0; j0 < pc.w; j0 += 4) {
+              T acc[4] = {T(0), T(0), T(0), T(0)};
+              const T *R = rhoB + pc.rho + j0;
+              for (int k0 = 0; k0 < pc.nr; k0 += 8) {
+                T ck[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) ck[k] = (k0 + k < pc.nr) ? C[(int64_t)dar * (k0 + k)] : T(0);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                  if (k0 + k < pc.nr) {
+                    const T *Rk = R + (int64_t)pc.ld * (k0 + k);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                      if (j0 + q < pc.w) acc[q] = fma(ck[k], __ldg(Rk + q), acc[q]);
+                  }
+                }
+              }
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (j0 + q < pc.w) Yr[pc.cs + j0 + q] = acc[q];
             }
           }
         }
-        __syncwarp();
+        __syncthreads();
+        mark(0);
+        // ---- stage 2: warp items (P_r, <= IR rows); lane = (row lrow, column lc) ----
+        for (int it = bt.it_begin + warp; it < bt.it_end; it += PN_WARPS) {
+          const PrWork pw = prwork[it];
+          const int na = pw.a_end - pw.a_begin;
+          AOp my_op = {0, 0, 0, 0, 0};
+          if (lane < na) my_op = aops[pw.a_begin + lane];
+          T *z = zs + (size_t)warp * (MAXA * 32);
+          const bool ok = lrow < pw.nr;
+          const T *Yc = ybuf + (pw.row0 - bt.row0 + (ok ? lrow : 0)) * CHP + lc;
+          if (np <= 16)
+            pn_mix<T, 16>(Yc, pstride, np, cov_s, lc, ok, ws, my_op.wrow, na, z + lane);
+          else
+            pn_mix<T, 32>(Yc, pstride, np, cov_s, lc, ok, ws, my_op.wrow, na, z + lane);
+          __syncwarp();
+          for (int ai = 0; ai < na; ++ai) {
+            const int64_t a_rho = __shfl_sync(0xffffffffu, my_op.rho, ai);
+            const int a_ld = __shfl_sync(0xffffffffu, my_op.ld, ai);
+            const int a_row0 = __shfl_sync(0xffffffffu, my_op.out_row0, ai);
+            const int a_nl = __shfl_sync(0xffffffffu, my_op.nl, ai);
+            const T *zr = z + ai * 32 + lc;  // z of (row r, column lc) sits at lane r*CH + lc
+            if (lc < nq) {
+              for (int l = lrow; l < a_nl; l += IR) {
+                const T *ra = rhoA + a_rho + l;
+                T rv[IR];
+#pragma unroll
+                for (int r = 0; r < IR; ++r) rv[r] = r < pw.nr ? __ldg(ra + (int64_t)a_ld * r) : T(0);
+                T v = T(0);
+#pragma unroll
+                for (int r = 0; r < IR; ++r)
+                  if (r < pw.nr) v = fma(rv[r], zr[r * CH], v);
+                atomicAdd(out_s + (a_row0 + l) + ldo * lc, v);
+              }
+            }
+          }
+          __syncwarp();
+        }
+        __syncthreads();  // ybuf is rewritten by the next batch; ws/sidx/cov by the next group
+        mark(2);
       }
-      __syncthreads();  // scratch, ws, sidx_s, cov_s are rewritten by the next group
     }
     for (int e = threadIdx.x; e < dal * nq; e += blockDim.x) {
       const int r = e % dal, c = e / dal;
       out[t.out + r + (int64_t)dal * c] += out_s[r + ldo * c];
     }
     __syncthreads();
+    mark(3);
   }
+  if (cycles && threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) atomicAdd(cycles + k, cyc[k]);
 }
 
 __global__ void k_d2f(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
@@ -264,7 +302,7 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t pn_smem(const PnPlan &P, size_t es) { return PnLayout(es, P.max_dal, P.CH).total; }
+static size_t pn_smem(const PnPlan &P, size_t es) { return PnLayout(es, P.max_dal, P.CH, P.batch_rows).total; }
 
 template <typename T>
 static void upload_pn(nsx_handle *h, const PnPlan &P, PnDevice &D) {
@@ -273,15 +311,16 @@ static void upload_pn(nsx_handle *h, const PnPlan &P, PnDevice &D) {
   D.tsrcs = dev_copy_pod(P.tsrcs);
   D.pieces = dev_copy_pod(P.pieces);
   D.prwork = dev_copy_pod(P.prwork);
+  D.batches = dev_copy_pod(P.batches);
   D.aops = dev_copy_pod(P.aops);
   D.tasks = dev_copy_pod(P.tasks);
   D.weights = dev_copy<T>(P.weights);
   int sms = 0;
   NSX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   D.grid = std::max(1, std::min<int>(sms, (int)P.tasks.size()));
-  size_t slot = (size_t)std::max(P.max_nsrc, 1) * P.CH * std::max(P.max_dar, 1);
-  NSX_CUDA(cudaMalloc(&D.scratch, slot * sizeof(T) * D.grid));
   NSX_CUDA(cudaMalloc(&D.counter, sizeof(int)));
+  NSX_CUDA(cudaMalloc(&D.cycles, 4 * sizeof(unsigned long long)));
+  NSX_CUDA(cudaMemset(D.cycles, 0, 4 * sizeof(unsigned long long)));
   D.smem = pn_smem(P, sizeof(T));
   if (D.smem > 227 * 1024) fail(NSX_E_ARG, "k_pn shared-memory layout exceeds 227 KB (output block too tall)");
 }
@@ -385,11 +424,10 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!P.tasks.empty()) {
     NSX_CUDA(cudaMemsetAsync(D.counter, 0, sizeof(int), s));
-    size_t slot = (size_t)std::max(P.max_nsrc, 1) * P.CH * std::max(P.max_dar, 1);
     StageScope sc(h, 1, s);
     k_pn<T, CH><<<D.grid, 512, D.smem, s>>>(D.tasks, (int)P.tasks.size(), D.tgroups, D.groups, D.tsrcs, D.pieces,
-                                            D.prwork, D.aops, (const T *)D.weights, x, rhoA, rhoB, out,
-                                            (T *)D.scratch, (int64_t)slot, D.counter, P.max_dal);
+                                            D.prwork, D.batches, D.aops, (const T *)D.weights, x, rhoA, rhoB, out,
+                                            D.counter, P.max_dal, P.batch_rows, h->timing ? D.cycles : nullptr);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -418,7 +456,8 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
 }
 
 static void free_pn(PnDevice &D) {
-  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.pieces, D.prwork, D.aops, D.tasks, D.weights, D.scratch, D.counter};
+  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.pieces, D.prwork, D.batches, D.aops, D.tasks, D.weights,
+                  D.counter, D.cycles};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   D = PnDevice();

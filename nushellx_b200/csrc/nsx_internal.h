@@ -72,6 +72,11 @@ struct Group {              // (output block, J_ar, lam): shared by the block's 
   int32_t na;               // proton operators of the group (weight rows)
   int32_t w_off;            // weights [na][nsrc], row-major
   int32_t pr_begin, pr_end; // range in prwork
+  int32_t bt_begin, bt_end; // range in batches (row batches of the group's items)
+};
+struct Batch {              // consecutive work items whose rows fit one shared-memory row batch
+  int32_t it_begin, it_end; // range in prwork
+  int32_t row0, nrows;      // proton rows [row0, row0 + nrows), nrows <= batch_rows
 };
 struct TGroup {             // a group as seen by one task: the sources present at Q_l
   int32_t grp;
@@ -105,11 +110,13 @@ struct PnTask {             // output block, CH consecutive neutron states (colu
 struct PnPlan {
   int CH = 8;
   int item_rows = 4;        // = 32 / CH: one row per lane in stage 2
+  int batch_rows = 64;      // proton rows of Y held in shared memory at a time
   std::vector<Group> groups;
   std::vector<TGroup> tgroups;
   std::vector<TSrc> tsrcs;
   std::vector<Piece> pieces;
   std::vector<PrWork> prwork;
+  std::vector<Batch> batches;
   std::vector<AOp> aops;
   std::vector<PnTask> tasks;
   std::vector<double> task_cost;
@@ -122,11 +129,12 @@ struct PnDevice {           // device copy of one plan (typed operand data lives
   TSrc *tsrcs = nullptr;
   Piece *pieces = nullptr;
   PrWork *prwork = nullptr;
+  Batch *batches = nullptr;
   AOp *aops = nullptr;
   PnTask *tasks = nullptr;
   void *weights = nullptr;  // T[]
-  void *scratch = nullptr;  // T[grid][max_nsrc][CH][max_dar]
   int *counter = nullptr;
+  unsigned long long *cycles = nullptr;  // [4] sub-stage SM cycles (timing only)
   int grid = 0;
   size_t smem = 0;
 };
@@ -186,6 +194,6 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], doub
 void flush_stage_events(nsx_handle *h);
 double sixj(int a, int b, int c, int d, int e, int f);
 std::vector<TabRow> pn_table(const nsx_handle *h);
-void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH, PnPlan &P);
+void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH, int batch_rows, PnPlan &P);
 double racah_w(int j1, int j2, int j3, int j4, int J, int K);
 }  // namespace nsx

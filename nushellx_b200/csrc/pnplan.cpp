@@ -74,10 +74,11 @@ std::vector<TabRow> pn_table(const nsx_handle *h) {
   return rows;
 }
 
-void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH, PnPlan &P) {
+void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH, int batch_rows, PnPlan &P) {
   const SpeciesPlan &A = h->A, &B = h->B;
   P = PnPlan();
   P.CH = CH;
+  P.batch_rows = batch_rows;
   P.item_rows = 32 / CH;
   const int IR = P.item_rows;
   // per b-key: left partition -> (right partition, value offset)
@@ -157,6 +158,23 @@ void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH
           }
         }
         G.pr_end = (int)P.prwork.size();
+        // row batches: maximal runs of items whose rows fit batch_rows (items are in row order)
+        G.bt_begin = (int)P.batches.size();
+        for (int it = G.pr_begin; it < G.pr_end;) {
+          Batch b;
+          b.it_begin = it;
+          b.row0 = P.prwork[it].row0;
+          int end_row = b.row0;
+          while (it < G.pr_end && P.prwork[it].row0 + P.prwork[it].nr - b.row0 <= batch_rows &&
+                 P.prwork[it].row0 >= b.row0) {
+            end_row = std::max(end_row, P.prwork[it].row0 + P.prwork[it].nr);
+            ++it;
+          }
+          b.it_end = it;
+          b.nrows = end_row - b.row0;
+          P.batches.push_back(b);
+        }
+        G.bt_end = (int)P.batches.size();
         gids.push_back((int)P.groups.size());
         gsrc.push_back(std::vector<std::pair<int, int>>(srcs.begin() + s0, srcs.begin() + s1));
         P.groups.push_back(G);

@@ -226,8 +226,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       h->flops_mix += 2.0 * nr * ob.db * r.e.size();
     }
   }
-  build_pn_plan(h, table, 8, h->pn64);   // FP64: 8 columns per task
-  build_pn_plan(h, table, 16, h->pn32);  // FP32: 16 columns per task
+  build_pn_plan(h, table, 8, 32, h->pn64);   // FP64: 8 columns per task, 32-row batches
+  build_pn_plan(h, table, 16, 64, h->pn32);  // FP32: 16 columns per task, 64-row batches
 }
 
 double racah_weight_ext(int Jal, int Jbl, int Jar, int Jbr, int J, int lam) {
