@@ -149,8 +149,8 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
               nsx_report *report);
 
 /* Device-side statistics of a handle (for benchmarking and profiling).
- * Stages of one H.v: 0 = like-particle products (k_like), 1 = fused pn
- * product (k_pn), 2 = unused, 3 = FP64 <-> FP32 conversions.
+ * Stages of one H.v: 0 = like-particle GEMMs (k_like), 1 = neutron-side Y
+ * products (k_y), 2 = mixing + proton side (k_a), 3 = precision conversion.
  * With timing enabled every stage launch is bracketed by CUDA events on its
  * stream; nsx_get_stats synchronises and sums them. */
 typedef struct nsx_stats {
@@ -160,8 +160,6 @@ typedef struct nsx_stats {
   double stage_ms[4];         /* summed device time per stage (timing enabled only) */
   double stage_bytes[4];      /* algorithmic HBM bytes of one launch of each stage  */
   double stage_flops[4];      /* algorithmic flops of one launch of each stage      */
-  double pn_cycles[4];        /* k_pn SM cycles summed over CTAs (timing enabled):
-                                 Y operands, weights, mixing + proton side, epilogue */
 } nsx_stats;
 
 /* Reset the counters; enable (1) or disable (0) per-stage event timing. */

@@ -152,8 +152,6 @@ int nsx_stats_reset(nsx_handle *h, int32_t timing) {
       h->stage_ms[i] = 0;
     }
     h->timing = timing != 0;
-    for (PnDevice *D : {&h->d.pn64, &h->d.pn32})
-      if (D->cycles) NSX_CUDA(cudaMemset(D->cycles, 0, 4 * sizeof(unsigned long long)));
   });
 }
 
@@ -170,13 +168,6 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
     for (int i = 0; i < 4; ++i) {
       out->stage_launches[i] = h->stage_launches[i];
       out->stage_ms[i] = h->stage_ms[i];
-      out->pn_cycles[i] = 0;
-    }
-    const PnDevice &D = prec == NSX_FP64 ? h->d.pn64 : h->d.pn32;
-    if (D.cycles) {
-      unsigned long long c[4];
-      NSX_CUDA(cudaMemcpy(c, D.cycles, sizeof(c), cudaMemcpyDeviceToHost));
-      for (int i = 0; i < 4; ++i) out->pn_cycles[i] = (double)c[i];
     }
   });
 }

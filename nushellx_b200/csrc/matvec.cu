@@ -3,22 +3,15 @@
 // The reference computes the product as multiplyx (pn), multiplya (pp) and
 // multiplyb (nn) in src/NuLnz/NuCoreX.f90:76-226 with axpy loops over density
 // sub-blocks (src/NuCommonX/NuCommonX.f90:745-919, 1009-1104).  Here it is
-// two stream-ordered kernels; every output element is owned by one CTA (no
-// global atomics, no per-thread copies of the vector):
+// three stream-ordered kernels, each output element owned by exactly one CTA
+// (no atomics, no per-thread vector copies):
 //
 //   k_like : out_b  = H_pp(Ja) C_b + C_b H_nn(Jb)              (dense tiled GEMM)
-//   k_pn   : persistent; a CTA owns the output columns of one neutron partition
-//            Q_l (a chunk of CH states) of one block and, for every (J_ar, lam)
-//            group of the pn table,
-//            in batches of at most 64 (FP32) / 32 (FP64) proton rows:
-//              stage 1: Y_(h,b)[batch rows, chunk] = C_h[rows, Q_r cols] rho_b[chunk, Q_r]^T
-//                       straight into shared memory (Y never leaves the SM);
-//              stage 2: per proton partition P_r (32/CH rows per warp item, one
-//                       element per lane) the sources are mixed in registers,
-//                       Z_a = sum w_(a,s) Y_s, and out[P_l rows] += rho_a[P_l, P_r] Z_a
-//                       is accumulated in shared memory.
-//            Each Y_(h,b) element is computed once (the reference recomputes the
-//            neutron-side product for every proton operator).
+//   k_y    : Y_(h,k) = C_h rho_k^T for every (input block h, neutron density k)
+//            that the pn table uses -- computed once and reused by every proton
+//            operator, where the reference recomputes it per proton operator;
+//   k_a    : out[P_l rows] += sum_(a,P_r) rho_a[P_l,P_r] (sum_k w_ak Y_(h,k)[P_r rows])
+//            (mixing of the Y intermediates fused into the operand load).
 //
 // Templated on the contraction type: double (the FP64 form) or float (the FP32
 // form, FP64 vectors converted at the boundary).
@@ -89,187 +82,112 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_pn: see the file comment.  512 threads (16 warps), one CTA per SM.
-//   shared Y batch layout: ybuf[p][row - batch row0][c] with odd row stride CH + 1
-//   stage-2 lane map: column c = lane % CH, row lane / CH (32 / CH rows per item)
-constexpr int PN_WARPS = 16;
-struct PnLayout {  // byte offsets of the k_pn shared-memory arrays (16-byte aligned)
-  size_t out, z, w, src, y, total;
-  __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ static int ldo(int dal) { return dal | 1; }  // odd: conflict-free column stride
-  __host__ __device__ PnLayout(size_t es, int max_dal, int ch, int batch_rows) {
-    out = 0;
-    z = al(out + es * (size_t)ldo(max_dal) * ch);
-    w = al(z + es * (size_t)PN_WARPS * MAXA * 32);
-    src = al(w + es * (size_t)MAXA * MAXS);
-    y = al(src + sizeof(int) * 2 * (size_t)MAXS);
-    total = al(y + es * (size_t)MAXS * batch_rows * (ch + 1));
-  }
-};
-
-// Stage-2 mixing of one lane's element: z_a = sum_p W[a][p] y_p for the item's
-// operators, y_p read once into registers (NP = 16 or 32 sources, zero-padded).
-template <typename T, int NP>
-__device__ __forceinline__ void pn_mix(const T *Yc, int pstride, int np, const uint32_t *cov, int lc, bool ok,
-                                       const T *ws, int my_wrow, int na, T *zrow) {
-  T y[NP];
-#pragma unroll
-  for (int p = 0; p < NP; ++p) y[p] = (ok && p < np && ((cov[p] >> lc) & 1u)) ? Yc[p * pstride] : T(0);
-  for (int ai = 0; ai < na; ++ai) {
-    const T *wr = ws + __shfl_sync(0xffffffffu, my_wrow, ai) * MAXS;
-    T zz = T(0);
-#pragma unroll
-    for (int p = 0; p < NP; ++p) zz = fma(wr[p], y[p], zz);
-    zrow[ai * 32] = zz;
+// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
+// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T.
+template <typename T>
+__global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
+                                           const T *__restrict__ x, const T *__restrict__ rho,
+                                           T *__restrict__ Y, int max_nr, int max_nl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
+  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
+  const YGroup g = groups[blockIdx.x];
+  const int row = g.row0 + threadIdx.x;
+  const bool active = row < g.m;
+  const T *C = x + g.c_base;
+  T *Yg = Y + g.y_base;
+  for (int bi = g.b_begin; bi < g.b_end; ++bi) {
+    const YBlk b = blks[bi];
+    const int n = b.nl * b.nr;
+    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
+    if (active)
+      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
+    __syncthreads();
+    if (active) {
+      for (int l = 0; l < b.nl; ++l) {
+        T acc = T(0);
+        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
+        Yg[row + (int64_t)g.m * (b.ycol + l)] = acc;
+      }
+    }
+    __syncthreads();
   }
 }
 
-template <typename T, int CH>
-__global__ void __launch_bounds__(512, 1)
-    k_pn(const PnTask *__restrict__ tasks, int ntasks, const TGroup *__restrict__ tgroups,
-         const Group *__restrict__ groups, const TSrc *__restrict__ tsrcs, const Piece *__restrict__ pieces,
-         const PrWork *__restrict__ prwork, const Batch *__restrict__ batches, const AOp *__restrict__ aops,
-         const T *__restrict__ W, const T *__restrict__ x, const T *__restrict__ rhoA, const T *__restrict__ rhoB,
-         T *__restrict__ out, int *__restrict__ counter, int max_dal, int batch_rows,
-         unsigned long long *__restrict__ cycles) {
-  constexpr int IR = 32 / CH;              // rows per work item: one (row, column) element per lane
-  constexpr int CHP = CH + 1;              // padded row stride of the Y batch (odd)
-  extern __shared__ __align__(16) unsigned char smem[];
-  const PnLayout L(sizeof(T), max_dal, CH, batch_rows);
-  T *out_s = reinterpret_cast<T *>(smem + L.out);   // [CH][ldo] : out_s[row + ldo*c]
-  T *zs = reinterpret_cast<T *>(smem + L.z);        // [warp][MAXA][32 lanes]
-  T *ws = reinterpret_cast<T *>(smem + L.w);        // [MAXA][MAXS] weights of the present sources (0-padded)
-  int *sidx_s = reinterpret_cast<int *>(smem + L.src);            // [MAXS]
-  uint32_t *cov_s = reinterpret_cast<uint32_t *>(sidx_s + MAXS);  // [MAXS]
-  T *ybuf = reinterpret_cast<T *>(smem + L.y);      // [p][batch row][CHP]
-  const int pstride = batch_rows * CHP;
-  __shared__ int s_task;
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int lc = lane % CH, lrow = lane / CH;
-  unsigned long long cyc[4] = {0, 0, 0, 0};
-  long long t0 = clock64();
-  auto mark = [&](int k) {
-    if (cycles && threadIdx.x == 0) {
-      long long t1 = clock64();
-      cyc[k] += (unsigned long long)(t1 - t0);
-      t0 = t1;
-    }
-  };
-  for (;;) {
-    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
-    __syncthreads();
-    const int ti = s_task;
-    __syncthreads();
-    if (ti >= ntasks) break;
-    const PnTask t = tasks[ti];
-    const int dal = t.d_al, nq = t.nq, ldo = PnLayout::ldo(dal);
-    for (int e = threadIdx.x; e < ldo * CH; e += blockDim.x) out_s[e] = T(0);
-    for (int gi = t.g_begin; gi < t.g_end; ++gi) {
-      const TGroup tg = tgroups[gi];
-      const Group G = groups[tg.grp];
-      const int np = tg.src_end - tg.src_begin;
-      const int dar = G.d_ar;
-      for (int e = threadIdx.x; e < MAXS; e += blockDim.x) {
-        if (e < np) {
-          const TSrc src = tsrcs[tg.src_begin + e];
-          sidx_s[e] = src.sidx;
-          cov_s[e] = src.cover;
-        } else {
-          sidx_s[e] = 0;
-          cov_s[e] = 0u;
-        }
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < G.na * MAXS; e += blockDim.x) {
-        const int a = e / MAXS, p = e - a * MAXS;
-        ws[e] = p < np ? W[G.w_off + a * G.nsrc + sidx_s[p]] : T(0);
-      }
-      mark(1);
-      for (int bi = G.bt_begin; bi < G.bt_end; ++bi) {
-        const Batch bt = batches[bi];
-        // ---- stage 1: Y_p[row][c] for the batch rows, into shared memory ----
-        for (int e = threadIdx.x; e < np * bt.nrows; e += blockDim.x) {
-          const int p = e / bt.nrows, rr = e - p * bt.nrows;
-          const int r = bt.row0 + rr;
-          const TSrc src = tsrcs[tg.src_begin + p];
-          T *Yr = ybuf + p * pstride + rr * CHP;
-          for (int pi = src.piece_begin; pi < src.piece_end; ++pi) {
-            const Piece pc = pieces[pi];
-            const T *C = x + pc.c + r;
-            for (int j0 = 0; j0 < pc.w; j0 += 4) {
-              T acc[4] = {T(0), T(0), T(0), T(0)};
-              const T *R = rhoB + pc.rho + j0;
-              for (int k0 = 0; k0 < pc.nr; k0 += 8) {
-                T ck[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) ck[k] = (k0 + k < pc.nr) ? C[(int64_t)dar * (k0 + k)] : T(0);
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                  if (k0 + k < pc.nr) {
-                    const T *Rk = R + (int64_t)pc.ld * (k0 + k);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                      if (j0 + q < pc.w) acc[q] = fma(ck[k], __ldg(Rk + q), acc[q]);
-                  }
-                }
-              }
-#pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (j0 + q < pc.w) Yr[pc.cs + j0 + q] = acc[q];
-            }
-          }
-        }
-        __syncthreads();
-        mark(0);
-        // ---- stage 2: warp items (P_r, <= IR rows); lane = (row lrow, column lc) ----
-        for (int it = bt.it_begin + warp; it < bt.it_end; it += PN_WARPS) {
-          const PrWork pw = prwork[it];
-          const int na = pw.a_end - pw.a_begin;
-          AOp my_op = {0, 0, 0, 0, 0};
-          if (lane < na) my_op = aops[pw.a_begin + lane];
-          T *z = zs + (size_t)warp * (MAXA * 32);
-          const bool ok = lrow < pw.nr;
-          const T *Yc = ybuf + (pw.row0 - bt.row0 + (ok ? lrow : 0)) * CHP + lc;
-          if (np <= 16)
-            pn_mix<T, 16>(Yc, pstride, np, cov_s, lc, ok, ws, my_op.wrow, na, z + lane);
-          else
-            pn_mix<T, 32>(Yc, pstride, np, cov_s, lc, ok, ws, my_op.wrow, na, z + lane);
-          __syncwarp();
-          for (int ai = 0; ai < na; ++ai) {
-            const int64_t a_rho = __shfl_sync(0xffffffffu, my_op.rho, ai);
-            const int a_ld = __shfl_sync(0xffffffffu, my_op.ld, ai);
-            const int a_row0 = __shfl_sync(0xffffffffu, my_op.out_row0, ai);
-            const int a_nl = __shfl_sync(0xffffffffu, my_op.nl, ai);
-            const T *zr = z + ai * 32 + lc;  // z of (row r, column lc) sits at lane r*CH + lc
-            if (lc < nq) {
-              for (int l = lrow; l < a_nl; l += IR) {
-                const T *ra = rhoA + a_rho + l;
-                T rv[IR];
-#pragma unroll
-                for (int r = 0; r < IR; ++r) rv[r] = r < pw.nr ? __ldg(ra + (int64_t)a_ld * r) : T(0);
-                T v = T(0);
-#pragma unroll
-                for (int r = 0; r < IR; ++r)
-                  if (r < pw.nr) v = fma(rv[r], zr[r * CH], v);
-                atomicAdd(out_s + (a_row0 + l) + ldo * lc, v);
-              }
-            }
-          }
-          __syncwarp();
-        }
-        __syncthreads();  // ybuf is rewritten by the next batch; ws/sidx/cov by the next group
-        mark(2);
-      }
-    }
-    for (int e = threadIdx.x; e < dal * nq; e += blockDim.x) {
-      const int r = e % dal, c = e / dal;
-      out[t.out + r + (int64_t)dal * c] += out_s[r + ldo * c];
-    }
-    __syncthreads();
-    mark(3);
+// ---------------------------------------------------------------------------
+// k_a: one CTA per output tile (block, P_l, <=64 columns); 256 threads own the
+// nl x ncols outputs (idx = tid + 256 q).  Per contribution: Z = sum w Y rows
+// (mixing) in shared memory, then acc += rho_a Z.
+constexpr int AQ = 16;  // outputs per thread: supports nl <= 64 with 64 columns
+struct KaLayout {  // byte offsets of the k_a shared-memory arrays (16-byte aligned)
+  size_t rs, zs, ws, ys, ls, total;
+  __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
+  __host__ __device__ KaLayout(size_t es, int nl, int nr, int nm) {
+    rs = 0;
+    zs = al(rs + es * (size_t)nl * nr);
+    ws = al(zs + es * (size_t)nr * 64);
+    ys = al(ws + es * (size_t)nm);
+    ls = al(ys + 8 * (size_t)nm);
+    total = al(ls + 4 * (size_t)nm);
   }
-  if (cycles && threadIdx.x == 0)
-    for (int k = 0; k < 4; ++k) atomicAdd(cycles + k, cyc[k]);
+};
+template <typename T>
+__global__ void __launch_bounds__(256) k_a(const ATile *__restrict__ tiles, const AContrib *__restrict__ contribs,
+                                           const AMix *__restrict__ mixes, const T *__restrict__ wts,
+                                           const T *__restrict__ rho, const T *__restrict__ Y, T *__restrict__ out,
+                                           int max_nr, int max_nl, int max_mix) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  KaLayout L(sizeof(T), max_nl, max_nr, max_mix);
+  T *rs = reinterpret_cast<T *>(smem_raw + L.rs);        // [max_nl*max_nr]
+  T *zs = reinterpret_cast<T *>(smem_raw + L.zs);        // [max_nr][64]
+  T *ws = reinterpret_cast<T *>(smem_raw + L.ws);        // [max_mix]
+  int64_t *ys = reinterpret_cast<int64_t *>(smem_raw + L.ys);  // [max_mix]
+  int *ls = reinterpret_cast<int *>(smem_raw + L.ls);    // [max_mix]
+  const ATile t = tiles[blockIdx.x];
+  const int nl = t.nl, ncols = t.ncols;
+  T acc[AQ];
+#pragma unroll
+  for (int q = 0; q < AQ; ++q) acc[q] = T(0);
+  for (int ci = t.c_begin; ci < t.c_end; ++ci) {
+    const AContrib c = contribs[ci];
+    const int nr = c.nr;
+    const int nm = c.m_end - c.m_begin;
+    for (int e = threadIdx.x; e < nl * nr; e += 256) rs[e] = rho[c.rho + e];
+    for (int e = threadIdx.x; e < nm; e += 256) {
+      const AMix m = mixes[c.m_begin + e];
+      ws[e] = wts[m.wi];
+      ys[e] = m.y;
+      ls[e] = m.ld;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * ncols; e += 256) {
+      const int k = e % nr, j = e / nr;
+      T z = T(0);
+      for (int m = 0; m < nm; ++m) z = fma(ws[m], Y[ys[m] + k + (int64_t)ls[m] * (t.col0 + j)], z);
+      zs[k * 64 + j] = z;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < AQ; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      const int i = idx % nl, j = idx / nl;
+      if (j < ncols) {
+        T a = acc[q];
+        for (int k = 0; k < nr; ++k) a = fma(rs[i + nl * k], zs[k * 64 + j], a);
+        acc[q] = a;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < AQ; ++q) {
+    const int idx = threadIdx.x + 256 * q;
+    const int i = idx % nl, j = idx / nl;
+    if (j < ncols) {
+      T *o = out + t.out + i + (int64_t)t.ld * j;
+      *o += acc[q];
+    }
+  }
 }
 
 __global__ void k_d2f(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
@@ -302,62 +220,65 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t pn_smem(const PnPlan &P, size_t es) { return PnLayout(es, P.max_dal, P.CH, P.batch_rows).total; }
-
-template <typename T>
-static void upload_pn(nsx_handle *h, const PnPlan &P, PnDevice &D) {
-  D.groups = dev_copy_pod(P.groups);
-  D.tgroups = dev_copy_pod(P.tgroups);
-  D.tsrcs = dev_copy_pod(P.tsrcs);
-  D.pieces = dev_copy_pod(P.pieces);
-  D.prwork = dev_copy_pod(P.prwork);
-  D.batches = dev_copy_pod(P.batches);
-  D.aops = dev_copy_pod(P.aops);
-  D.tasks = dev_copy_pod(P.tasks);
-  D.weights = dev_copy<T>(P.weights);
-  int sms = 0;
-  NSX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-  D.grid = std::max(1, std::min<int>(sms, (int)P.tasks.size()));
-  NSX_CUDA(cudaMalloc(&D.counter, sizeof(int)));
-  NSX_CUDA(cudaMalloc(&D.cycles, 4 * sizeof(unsigned long long)));
-  NSX_CUDA(cudaMemset(D.cycles, 0, 4 * sizeof(unsigned long long)));
-  D.smem = pn_smem(P, sizeof(T));
-  if (D.smem > 227 * 1024) fail(NSX_E_ARG, "k_pn shared-memory layout exceeds 227 KB (output block too tall)");
+static size_t ky_smem(const nsx_handle *h, size_t es) {
+  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
+}
+static size_t ka_smem(const nsx_handle *h, size_t es) {
+  return KaLayout(es, h->max_anl, h->max_anr, h->max_mix).total;
 }
 
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
+  if (h->max_anl > AQ * 256 / 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
-  for (const PnPlan *P : {&h->pn64, &h->pn32}) {
-    for (const Group &g : P->groups)
-      if (g.na > MAXA || g.nsrc > MAXS) fail(NSX_E_ARG, "pn group exceeds the k_pn operator/source limits");
-  }
   d.rhoA = dev_copy<double>(h->A.vals);
   d.rhoB = dev_copy<double>(h->B.vals);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
+  d.w = dev_copy<double>(h->weights);
+  d.ygroups = dev_copy_pod(h->ygroups);
+  d.yblks = dev_copy_pod(h->yblks);
+  d.atiles = dev_copy_pod(h->atiles);
+  d.acontribs = dev_copy_pod(h->acontribs);
+  d.amixes = dev_copy_pod(h->amixes);
   d.ltiles = dev_copy_pod(h->ltiles);
-  upload_pn<double>(h, h->pn64, d.pn64);
   NSX_CUDA(cudaMalloc(&d.xin, h->no_state * sizeof(double)));
   NSX_CUDA(cudaMalloc(&d.xout, h->no_state * sizeof(double)));
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
-  NSX_CUDA(cudaFuncSetAttribute(k_pn<double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.pn64.smem));
+  for (size_t es : {sizeof(double), sizeof(float)}) {
+    if (ky_smem(h, es) > 227 * 1024 || ka_smem(h, es) > 227 * 1024)
+      fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_y / k_a");
+  }
+  NSX_CUDA(cudaFuncSetAttribute(k_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 8)));
+  NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 8)));
+  NSX_CUDA(cudaFuncSetAttribute(k_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 4)));
+  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 4)));
 }
 
 void ensure_precision(nsx_handle *h, int precision) {
   auto &d = h->d;
-  if (precision == NSX_FP64) return;
-  if (precision != NSX_FP32) fail(NSX_E_ARG, "unknown precision");
-  if (d.x32) return;
-  d.rhoA32 = dev_copy<float>(h->A.vals);
-  d.rhoB32 = dev_copy<float>(h->B.vals);
-  d.hA32 = dev_copy<float>(h->A.hdense);
-  d.hB32 = dev_copy<float>(h->B.hdense);
-  upload_pn<float>(h, h->pn32, d.pn32);
-  NSX_CUDA(cudaFuncSetAttribute(k_pn<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.pn32.smem));
-  NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
-  NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
+  size_t ny = std::max<int64_t>(h->y_elems, 1);
+  if (precision == NSX_FP64) {
+    if (!d.y64) {
+      NSX_CUDA(cudaMalloc(&d.y64, ny * sizeof(double)));
+      NSX_CUDA(cudaMemset(d.y64, 0, ny * sizeof(double)));  // unreachable column slabs stay zero
+    }
+  } else if (precision == NSX_FP32) {
+    if (!d.y32) {
+      NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
+      NSX_CUDA(cudaMemset(d.y32, 0, ny * sizeof(float)));
+      d.rhoA32 = dev_copy<float>(h->A.vals);
+      d.rhoB32 = dev_copy<float>(h->B.vals);
+      d.hA32 = dev_copy<float>(h->A.hdense);
+      d.hB32 = dev_copy<float>(h->B.hdense);
+      d.w32 = dev_copy<float>(h->weights);
+      NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
+      NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
+    }
+  } else {
+    fail(NSX_E_ARG, "unknown precision");
+  }
 }
 
 // Brackets one stage launch with events when per-stage timing is enabled.
@@ -396,38 +317,39 @@ void flush_stage_events(nsx_handle *h) {
 }
 
 // Algorithmic traffic (each operand read once, each result written once) and
-// flops of one launch of each stage.  k_pn keeps its Y operands on chip/L2, so
-// its algorithmic bytes are the input vector, both density sets and the output.
+// flops of one launch of each stage.
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]) {
   const double es = precision == NSX_FP64 ? 8.0 : 4.0;
   const double n = (double)h->no_state;
   double rhoA = (double)h->A.vals.size(), rhoB = (double)h->B.vals.size();
   double hd = (double)(h->A.hdense.size() + h->B.hdense.size());
-  const PnPlan &P = precision == NSX_FP64 ? h->pn64 : h->pn32;
-  bytes[0] = es * (2.0 * n + hd);
-  bytes[1] = es * (3.0 * n + rhoA + rhoB + (double)P.weights.size());
-  bytes[2] = 0.0;
-  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);
+  bytes[0] = es * (2.0 * n + hd);                               // C in, out written, dense H
+  bytes[1] = es * (n + rhoB + (double)h->y_elems);              // C in, rho_B, Y written
+  bytes[2] = es * ((double)h->y_elems + rhoA + 2.0 * n) + 4.0 * (double)h->weights.size();  // Y, rho_A, out r/w
+  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);     // one conversion launch
   flops[0] = h->flops_like;
-  flops[1] = h->flops_y + h->flops_mix + h->flops_a;
-  flops[2] = 0.0;
+  flops[1] = h->flops_y;
+  flops[2] = h->flops_mix + h->flops_a;
   flops[3] = 0.0;
 }
 
-template <typename T, int CH>
+template <typename T>
 static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T *rhoB, const T *hA, const T *hB,
-                       const PnPlan &P, const PnDevice &D, cudaStream_t s) {
+                       const T *w, T *Y, cudaStream_t s) {
   auto &d = h->d;
   if (!h->ltiles.empty()) {
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
   }
-  if (!P.tasks.empty()) {
-    NSX_CUDA(cudaMemsetAsync(D.counter, 0, sizeof(int), s));
+  if (!h->ygroups.empty()) {
     StageScope sc(h, 1, s);
-    k_pn<T, CH><<<D.grid, 512, D.smem, s>>>(D.tasks, (int)P.tasks.size(), D.tgroups, D.groups, D.tsrcs, D.pieces,
-                                            D.prwork, D.batches, D.aops, (const T *)D.weights, x, rhoA, rhoB, out,
-                                            D.counter, P.max_dal, P.batch_rows, h->timing ? D.cycles : nullptr);
+    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
+                                                                             h->max_ynr, h->max_ynl);
+  }
+  if (!h->atiles.empty()) {
+    StageScope sc(h, 2, s);
+    k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(
+        d.atiles, d.acontribs, d.amixes, w, rhoA, Y, out, h->max_anr, h->max_anl, h->max_mix);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -438,7 +360,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   h->matvecs++;
   h->last_precision = precision;
   if (precision == NSX_FP64) {
-    run_stages<double, 8>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, h->pn64, d.pn64, s);
+    run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.y64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -446,7 +368,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       StageScope sc(h, 3, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float, 16>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, h->pn32, d.pn32, s);
+    run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.y32, s);
     {
       StageScope sc(h, 3, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
@@ -455,22 +377,12 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   }
 }
 
-static void free_pn(PnDevice &D) {
-  void *ptrs[] = {D.groups, D.tgroups, D.tsrcs, D.pieces, D.prwork, D.batches, D.aops, D.tasks, D.weights,
-                  D.counter, D.cycles};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
-  D = PnDevice();
-}
-
 void release(nsx_handle *h) {
   auto &d = h->d;
-  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.ltiles,
-                  d.x32, d.o32, d.xin, d.xout};
+  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.ygroups, d.yblks,
+                  d.atiles, d.acontribs, d.amixes, d.ltiles, d.y64, d.y32, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  free_pn(d.pn64);
-  free_pn(d.pn32);
   d = DeviceBuffers();
   for (auto &e : h->stage_events) {
     cudaEventDestroy(e.second.first);

@@ -53,92 +53,39 @@ struct Block {
   int64_t off;
 };
 
-// ---- pn table (drdbh) -----------------------------------------------------------
-struct TabEnt {
-  int bk, hb;       // neutron density key, input block
-  double w;         // V_lam * renorm * Racah weight
+// ---- task lists of the H.v kernels -------------------------------------------
+// Y stage: Y_(h,b) = C_h * rho_b^T, one group per (Y matrix, row tile).
+struct YGroup {
+  int64_t c_base;   // element offset of input block h
+  int64_t y_base;   // element offset of the Y matrix (d_ar x d_bl, column-major)
+  int32_t m;        // d_ar (rows, leading dimension of C_h and Y)
+  int32_t row0;     // first row of the tile
+  int32_t b_begin, b_end;  // range in yblks
 };
-struct TabRow {     // one (output block, J_ar, proton density key)
-  int bl, jar, ak, lam;
-  std::vector<TabEnt> e;
+struct YBlk {
+  int64_t rho;      // offset of the nl x nr (column-major) density sub-block
+  int32_t ccol;     // first column of C_h (right partition Q_r)
+  int32_t ycol;     // first column of Y (left partition Q_l)
+  int32_t nl, nr;
 };
-
-// ---- plan of the fused pn kernel k_pn ---------------------------------------------
-constexpr int MAXA = 16;    // proton operators per work item
-constexpr int MAXS = 32;    // sources (h, b) per group
-struct Group {              // (output block, J_ar, lam): shared by the block's tasks
-  int32_t d_ar;             // proton rows of the Y operands (d_a(J_ar))
-  int32_t nsrc;             // sources of the group (<= MAXS)
-  int32_t na;               // proton operators of the group (weight rows)
-  int32_t w_off;            // weights [na][nsrc], row-major
-  int32_t pr_begin, pr_end; // range in prwork
-  int32_t bt_begin, bt_end; // range in batches (row batches of the group's items)
+// A stage: output tile (block, left proton partition P_l, column range).
+struct ATile {
+  int64_t out;      // element offset of out[P_l row 0, col0] in the output vector
+  int32_t ld;       // d_al (leading dimension of the output block)
+  int32_t nl;       // rows of the tile = nJT(P_l, J_al)
+  int32_t col0, ncols;
+  int32_t c_begin, c_end;  // range in contribs
 };
-struct Batch {              // consecutive work items whose rows fit one shared-memory row batch
-  int32_t it_begin, it_end; // range in prwork
-  int32_t row0, nrows;      // proton rows [row0, row0 + nrows), nrows <= batch_rows
+struct AContrib {
+  int64_t rho;      // offset of the nl x nr proton density sub-block (column-major)
+  int32_t nr;       // nJT(P_r, J_ar)
+  int32_t m_begin, m_end;  // range in mixes
 };
-struct TGroup {             // a group as seen by one task: the sources present at Q_l
-  int32_t grp;
-  int32_t src_begin, src_end;
+struct AMix {
+  int64_t y;        // offset of Y_(h,b)[P_r row 0, col 0]
+  int32_t ld;       // d_ar (leading dimension of that Y matrix)
+  int32_t wi;       // index into the weight array
 };
-struct TSrc {               // a group source present in a task's column chunk
-  int32_t piece_begin, piece_end;  // range in pieces
-  uint32_t cover;           // chunk columns the pieces cover (bit c)
-  int32_t sidx;             // source index within the group
-};
-struct Piece {              // Y_s[:, cs..cs+w) = C_h[:, Q_r cols] rho_b[rows.., Q_r]^T
-  int64_t c;                // offset of C_h[0, first column of Q_r]
-  int64_t rho;              // offset of rho_b(Q_l, Q_r) element (first row of the piece, col 0)
-  int32_t ld;               // n(Q_l): leading dimension of the density block
-  int32_t nr;               // n(Q_r)
-  int32_t cs, w;            // chunk columns [cs, cs+w)
-};
-struct PrWork {             // <= item_rows rows of one proton right partition P_r
-  int32_t row0, nr;
-  int32_t a_begin, a_end;   // range in aops (<= MAXA)
-};
-struct AOp {                // proton density block rho_a(P_l, P_r), rows chunk of P_r
-  int64_t rho;              // offset of element (0, chunk row 0); block nl x n(P_r) column-major
-  int32_t ld, out_row0, nl, wrow;
-};
-struct PnTask {             // output block, CH consecutive neutron states (columns)
-  int64_t out;              // offset of out[row 0, first column]
-  int32_t d_al, nq;
-  int32_t g_begin, g_end;   // range in tgroups
-};
-struct PnPlan {
-  int CH = 8;
-  int item_rows = 4;        // = 32 / CH: one row per lane in stage 2
-  int batch_rows = 64;      // proton rows of Y held in shared memory at a time
-  std::vector<Group> groups;
-  std::vector<TGroup> tgroups;
-  std::vector<TSrc> tsrcs;
-  std::vector<Piece> pieces;
-  std::vector<PrWork> prwork;
-  std::vector<Batch> batches;
-  std::vector<AOp> aops;
-  std::vector<PnTask> tasks;
-  std::vector<double> task_cost;
-  std::vector<double> weights;
-  int max_dar = 0, max_dal = 0, max_nsrc = 0, max_nl = 0;
-};
-struct PnDevice {           // device copy of one plan (typed operand data lives in DeviceBuffers)
-  Group *groups = nullptr;
-  TGroup *tgroups = nullptr;
-  TSrc *tsrcs = nullptr;
-  Piece *pieces = nullptr;
-  PrWork *prwork = nullptr;
-  Batch *batches = nullptr;
-  AOp *aops = nullptr;
-  PnTask *tasks = nullptr;
-  void *weights = nullptr;  // T[]
-  int *counter = nullptr;
-  unsigned long long *cycles = nullptr;  // [4] sub-stage SM cycles (timing only)
-  int grid = 0;
-  size_t smem = 0;
-};
-
 // like-particle part: out_blk = Ha C + C Hb, 64x64 output tiles.
 struct LTile {
   int64_t c;        // block offset
@@ -148,10 +95,17 @@ struct LTile {
 };
 
 struct DeviceBuffers {
-  double *rhoA = nullptr, *rhoB = nullptr, *hA = nullptr, *hB = nullptr;
-  float *rhoA32 = nullptr, *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr;
+  // FP64 operator data
+  double *rhoA = nullptr, *rhoB = nullptr, *hA = nullptr, *hB = nullptr, *w = nullptr;
+  float *rhoA32 = nullptr, *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr, *w32 = nullptr;
+  YGroup *ygroups = nullptr;
+  YBlk *yblks = nullptr;
+  ATile *atiles = nullptr;
+  AContrib *acontribs = nullptr;
+  AMix *amixes = nullptr;
   LTile *ltiles = nullptr;
-  PnDevice pn64, pn32;
+  double *y64 = nullptr;   // Y intermediates, FP64
+  float *y32 = nullptr;    // Y intermediates, FP32
   float *x32 = nullptr, *o32 = nullptr;
   double *xin = nullptr, *xout = nullptr;  // host-API staging
 };
@@ -169,9 +123,15 @@ struct nsx_handle {
   // pn multipole interaction: key (sal, sar, sbl, sbr, lam) -> V * renorm
   std::unordered_map<uint64_t, double> vop;
   // plan
+  std::vector<nsx::YGroup> ygroups;
+  std::vector<nsx::YBlk> yblks;
+  std::vector<nsx::ATile> atiles;
+  std::vector<nsx::AContrib> acontribs;
+  std::vector<nsx::AMix> amixes;
+  std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
-  nsx::PnPlan pn64, pn32;   // CH = 8 (FP64) and CH = 16 (FP32)
-  int64_t y_elems = 0;      // Y operand elements of one H.v (algorithmic)
+  int64_t y_elems = 0;
+  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_anr = 0, max_mix = 0;
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -193,7 +153,5 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]);
 void flush_stage_events(nsx_handle *h);
 double sixj(int a, int b, int c, int d, int e, int f);
-std::vector<TabRow> pn_table(const nsx_handle *h);
-void build_pn_plan(const nsx_handle *h, const std::vector<TabRow> &table, int CH, int batch_rows, PnPlan &P);
 double racah_w(int j1, int j2, int j3, int j4, int J, int K);
 }  // namespace nsx

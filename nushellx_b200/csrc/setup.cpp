@@ -179,6 +179,17 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           for (int ka = 0; ka < A.njt_of(pa, b.J2a); ++ka, ++n)
             h->lcoef[n] = (p->parity == 0 || A.par[pa] * B.par[pb] == p->parity) ? 1 : 0;
   }
+  // key indices: a-keys by (Jl, Jr); b-keys by (Jl, Jr, lam)
+  std::map<std::pair<int, int>, std::vector<int>> akeys;
+  std::map<std::tuple<int, int, int>, std::vector<int>> bkeys;
+  for (int k = 0; k < (int)A.keys.size(); ++k) {
+    uint64_t key = A.keys[k];
+    akeys[{(int)(key & 255), (int)((key >> 8) & 255)}].push_back(k);
+  }
+  for (int k = 0; k < (int)B.keys.size(); ++k) {
+    uint64_t key = B.keys[k];
+    bkeys[{(int)(key & 255), (int)((key >> 8) & 255), (int)((key >> 32) & 255)}].push_back(k);
+  }
   // like-particle tiles and flops (segment count, src/NuCommonX/NuCommonX.f90:1009-1104)
   h->ltiles.clear();
   h->flops_like = 0;
@@ -200,38 +211,154 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     for (auto &b : h->blocks)
       if (b.J2b == J2s) h->flops_like += 2.0 * nn * b.da;
   }
-  // pn table and its algorithmic cost (reuse-aware: each Y_(h,b) once, mixing, proton side)
-  std::vector<TabRow> table = pn_table(h);
+
+  // ---- pn table (drdbh, src/NuLnz/NuCoreX.f90:1428-1577) ----------------------
+  // entries per (output block, J_ar, a-key): list of (b-key, input block, weight)
+  struct Entry { int bk, hb; double w; };
+  std::map<std::pair<int, int>, int> ymat;  // (input block, b-key) -> Y matrix index
+  std::vector<std::pair<int, int>> ymats;
+  std::vector<int64_t> yoff;
+  h->weights.clear();
+  h->ygroups.clear();
+  h->yblks.clear();
+  h->atiles.clear();
+  h->acontribs.clear();
+  h->amixes.clear();
   h->flops_y = h->flops_mix = h->flops_a = 0;
-  h->y_elems = 0;
-  std::map<std::pair<int, int>, int> seen;
-  for (const TabRow &r : table) {
-    const Block &ob = h->blocks[r.bl];
-    for (const TabEnt &e : r.e) {
-      if (!seen.count({e.hb, e.bk})) {
-        seen[{e.hb, e.bk}] = 1;
-        double nnz = 0, cols = 0;
-        int J2bl = (int)(B.keys[e.bk] & 255), J2br = (int)((B.keys[e.bk] >> 8) & 255);
-        for (const RhoBlk &rb : B.kblocks[e.bk]) {
-          nnz += (double)B.njt_of(rb.pl, J2bl) * B.njt_of(rb.pr, J2br);
-          cols += B.njt_of(rb.pl, J2bl);
+  int64_t ytot = 0;
+  auto get_ymat = [&](int hb, int bk) {
+    auto it = ymat.find({hb, bk});
+    if (it != ymat.end()) return it->second;
+    int id = (int)ymats.size();
+    ymat[{hb, bk}] = id;
+    ymats.push_back({hb, bk});
+    yoff.push_back(ytot);
+    int J2bl = (int)(B.keys[bk] & 255);
+    ytot += (int64_t)h->blocks[hb].da * B.dim(J2bl);
+    return id;
+  };
+  const int TW = 64;  // output columns per k_a tile
+  for (size_t bl = 0; bl < h->blocks.size(); ++bl) {
+    const Block &ob = h->blocks[bl];
+    if (ob.da == 0 || ob.db == 0) continue;
+    // contributions per left partition P_l
+    std::vector<std::vector<AContrib>> per_pl(A.nspart);
+    std::vector<std::vector<std::vector<AMix>>> per_pl_mix(A.nspart);
+    for (int jar = A.minJ2; jar <= A.maxJ2; jar += 2) {
+      auto ait = akeys.find({ob.J2a, jar});
+      if (ait == akeys.end()) continue;
+      for (int ak : ait->second) {
+        uint64_t akey = A.keys[ak];
+        int sal = (akey >> 16) & 255, sar = (akey >> 24) & 255, lam = (akey >> 32) & 255;
+        std::vector<Entry> ents;
+        int jbrn = std::max(std::abs(ob.J2b - lam), std::abs(jar - J2));
+        int jbrx = std::min(std::min(ob.J2b + lam, jar + J2), B.maxJ2);
+        for (int jbr = jbrn; jbr <= jbrx; jbr += 2) {
+          if (!B.has_J(jbr)) continue;
+          auto hit = bidx.find({jar, jbr});
+          if (hit == bidx.end()) continue;
+          const Block &ib = h->blocks[hit->second];
+          if (ib.da == 0 || ib.db == 0) continue;
+          double rw = racah_weight(ob.J2a, ob.J2b, jar, jbr, J2, lam);
+          if (rw == 0.0) continue;
+          auto bit = bkeys.find({ob.J2b, jbr, lam});
+          if (bit == bkeys.end()) continue;
+          for (int bk : bit->second) {
+            uint64_t bkey = B.keys[bk];
+            int sbl = (bkey >> 16) & 255, sbr = (bkey >> 24) & 255;
+            auto vit = h->vop.find(pack_key(sal, sar, sbl, sbr, lam));
+            if (vit == h->vop.end() || vit->second == 0.0) continue;
+            if (B.kblocks[bk].empty()) continue;
+            ents.push_back({bk, hit->second, vit->second * rw});
+          }
         }
-        h->flops_y += 2.0 * h->blocks[e.hb].da * nnz;
-        h->y_elems += (int64_t)h->blocks[e.hb].da * (int64_t)cols;
+        if (ents.empty() || A.kblocks[ak].empty()) continue;
+        for (const RhoBlk &rb : A.kblocks[ak]) {
+          if (rb.pl >= A.nspart) continue;
+          int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
+          AContrib c;
+          c.rho = rb.voff;
+          c.nr = nr;
+          std::vector<AMix> mx;
+          for (const Entry &e : ents) {
+            int yid = get_ymat(e.hb, e.bk);
+            AMix m;
+            m.y = yoff[yid] + A.poff[A.jidx(jar)][rb.pr];
+            m.ld = h->blocks[e.hb].da;
+            m.wi = (int)h->weights.size();
+            h->weights.push_back(e.w);
+            mx.push_back(m);
+          }
+          per_pl[rb.pl].push_back(c);
+          per_pl_mix[rb.pl].push_back(std::move(mx));
+          h->flops_a += 2.0 * nl * nr * ob.db;
+          h->flops_mix += 2.0 * nr * ob.db * ents.size();
+        }
       }
     }
-    for (const RhoBlk &rb : A.kblocks[r.ak]) {
-      double nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, r.jar);
-      h->flops_a += 2.0 * nl * nr * ob.db;
-      h->flops_mix += 2.0 * nr * ob.db * r.e.size();
+    std::vector<ATile> btiles;  // this output block's tiles, reordered below
+    for (int pl = 0; pl < A.nspart; ++pl) {
+      int nl = A.njt_of(pl, ob.J2a);
+      if (nl == 0 || per_pl[pl].empty()) continue;
+      int cb = (int)h->acontribs.size();
+      for (size_t i = 0; i < per_pl[pl].size(); ++i) {
+        AContrib c = per_pl[pl][i];
+        c.m_begin = (int)h->amixes.size();
+        for (auto &m : per_pl_mix[pl][i]) h->amixes.push_back(m);
+        c.m_end = (int)h->amixes.size();
+        h->acontribs.push_back(c);
+      }
+      int ce = (int)h->acontribs.size();
+      for (int c0 = 0; c0 < ob.db; c0 += TW) {
+        ATile t;
+        t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
+        t.ld = ob.da;
+        t.nl = nl;
+        t.col0 = c0;
+        t.ncols = std::min(TW, ob.db - c0);
+        t.c_begin = cb;
+        t.c_end = ce;
+        btiles.push_back(t);
+      }
     }
+    // Tiles of the same column range are launched next to each other: they mix the same
+    // Y column slabs (all proton rows P_r) in the same contribution order, so their reads
+    // meet in L2 instead of each going to DRAM.
+    std::stable_sort(btiles.begin(), btiles.end(), [](const ATile &x, const ATile &y) { return x.col0 < y.col0; });
+    h->atiles.insert(h->atiles.end(), btiles.begin(), btiles.end());
   }
-  build_pn_plan(h, table, 8, 32, h->pn64);   // FP64: 8 columns per task, 32-row batches
-  build_pn_plan(h, table, 16, 64, h->pn32);  // FP32: 16 columns per task, 64-row batches
-}
-
-double racah_weight_ext(int Jal, int Jbl, int Jar, int Jbr, int J, int lam) {
-  return racah_weight(Jal, Jbl, Jar, Jbr, J, lam);
+  // Y groups: one per (Y matrix, 128-row tile), sharing the matrix's sub-block list
+  for (size_t y = 0; y < ymats.size(); ++y) {
+    int hb = ymats[y].first, bk = ymats[y].second;
+    const Block &ib = h->blocks[hb];
+    int J2bl = (int)(B.keys[bk] & 255), J2br = (int)((B.keys[bk] >> 8) & 255);
+    int b0 = (int)h->yblks.size();
+    double nnz = 0;
+    for (const RhoBlk &rb : B.kblocks[bk]) {
+      YBlk yb;
+      yb.rho = rb.voff;
+      yb.ccol = B.poff[B.jidx(J2br)][rb.pr];
+      yb.ycol = B.poff[B.jidx(J2bl)][rb.pl];
+      yb.nl = B.njt_of(rb.pl, J2bl);
+      yb.nr = B.njt_of(rb.pr, J2br);
+      nnz += (double)yb.nl * yb.nr;
+      h->yblks.push_back(yb);
+    }
+    int b1 = (int)h->yblks.size();
+    h->flops_y += 2.0 * ib.da * nnz;
+    for (int r0 = 0; r0 < ib.da; r0 += 128) h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1});
+  }
+  h->y_elems = ytot;
+  h->max_ynl = h->max_ynr = h->max_anl = h->max_anr = h->max_mix = 0;
+  for (auto &y : h->yblks) {
+    h->max_ynl = std::max(h->max_ynl, y.nl);
+    h->max_ynr = std::max(h->max_ynr, y.nr);
+  }
+  for (auto &t : h->atiles) h->max_anl = std::max(h->max_anl, t.nl);
+  for (auto &c : h->acontribs) {
+    h->max_anr = std::max(h->max_anr, c.nr);
+    h->max_mix = std::max(h->max_mix, c.m_end - c.m_begin);
+  }
 }
 
 }  // namespace nsx

@@ -55,17 +55,15 @@ class Report(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("launches", C.c_int64), ("matvecs", C.c_int64), ("stage_launches", C.c_int64 * 4),
-                ("stage_ms", C.c_double * 4), ("stage_bytes", C.c_double * 4), ("stage_flops", C.c_double * 4),
-                ("pn_cycles", C.c_double * 4)]
+                ("stage_ms", C.c_double * 4), ("stage_bytes", C.c_double * 4), ("stage_flops", C.c_double * 4)]
 
-    STAGES = ("k_like", "k_pn", "unused", "k_convert")
+    STAGES = ("k_like", "k_y", "k_a", "k_convert")
 
     def as_dict(self):
         return {"launches": self.launches, "matvecs": self.matvecs,
                 "stages": {n: {"launches": self.stage_launches[i], "ms": self.stage_ms[i],
                                "bytes": self.stage_bytes[i], "flops": self.stage_flops[i]}
-                           for i, n in enumerate(self.STAGES)},
-                "pn_cycles": [self.pn_cycles[i] for i in range(4)]}
+                           for i, n in enumerate(self.STAGES)}}
 
 
 class Files(C.Structure):

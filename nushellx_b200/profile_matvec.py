@@ -22,11 +22,7 @@ def main():
     S.stats_reset(timing=True)
     for _ in range(reps):
         S.matvec(x.data_ptr(), y.data_ptr(), prec)
-    allst = S.stats()
-    st = allst["stages"]
-    cyc = allst["pn_cycles"]
-    tot = sum(cyc) or 1.0
-    print("k_pn sub-stage cycle shares (Y, weights, mix+proton, epilogue):", [round(c / tot, 3) for c in cyc])
+    st = S.stats()["stages"]
     per = {k: round(v["ms"] / v["launches"], 4) for k, v in st.items() if v["launches"]}
     print(name, "dim", S.dim, "ok", float(y.abs().max()), "ms/launch", per)
     S.close()
