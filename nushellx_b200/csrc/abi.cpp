@@ -17,6 +17,7 @@ void check_cuda(cudaError_t e, const char *what) {
 }
 void solve(nsx_handle *h, const nsx_params *P, double *evals, double *evecs, nsx_report *rep);
 std::shared_ptr<void> load_files(const nsx_files *f, nsx_problem *p);
+int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 
 template <typename F>
 static int guarded(F &&f) {
@@ -121,6 +122,10 @@ int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, voi
     NSX_CUDA(cudaSetDevice(h->device));
     matvec_device(h, x, y, precision, (cudaStream_t)stream);
   });
+}
+
+int nsx_matvec_noalloc(nsx_handle *h, const double *x, double *y, void *stream) {
+  return guarded([&] { noalloc_guarded(h, x, y, stream); });
 }
 
 int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision) {

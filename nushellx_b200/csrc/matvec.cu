@@ -377,6 +377,14 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   }
 }
 
+// The FP64 stages with a caller-provided Y buffer (used by the fixed-scratch entry point).
+void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *Y, cudaStream_t s) {
+  auto &d = h->d;
+  h->matvecs++;
+  h->last_precision = NSX_FP64;
+  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, Y, s);
+}
+
 void release(nsx_handle *h) {
   auto &d = h->d;
   void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.ygroups, d.yblks,

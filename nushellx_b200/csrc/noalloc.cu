@@ -1,0 +1,64 @@
+// nsx_matvec_noalloc: the FP64 H.v with its scratch in a fixed device array.
+//
+// Why: nsx_matvec allocates its Y intermediates with cudaMalloc on the first
+// product of a handle.  Some callers cannot allow that during the call:
+// cudaMalloc synchronises the whole device (it would stall the caller's other
+// streams), and hosts that hand all device memory to their own pool allocator
+// leave nothing to allocate from.  This entry point allocates nothing; its Y
+// scratch is the file-scope array below, of a fixed maximum size.
+//
+// Rules for callers:
+// * The array holds NOALLOC_Y_MAX FP64 elements (64 MiB); a problem whose Y
+//   intermediates need more is rejected with NSX_E_ARG and a message.
+// * The first call on a device looks up the array's device address (this
+//   loads the library's module on that device if it is not loaded yet); make
+//   that first call before any stream capture.  Every GPU that loads the
+//   library holds the array until the process exits.
+// * All calls share the one array and it keeps the last call's contents; the
+//   part the product needs zeroed is cleared at the start of every call on the
+//   caller's stream.  Calls that overlap on the GPU (different streams, or
+//   different handles on the same device, without ordering) race on the array.
+#include <mutex>
+#include "nsx_internal.h"
+
+namespace nsx {
+
+constexpr int64_t NOALLOC_Y_MAX = int64_t(8) << 20;  // FP64 elements (64 MiB)
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_noalloc_y[NOALLOC_Y_MAX];
+
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_noalloc_y on the current device (looked up once per device).
+static double *noalloc_scratch(int device) {
+  if (device < 0 || device >= NOALLOC_MAX_DEVICES) fail(NSX_E_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_y);
+    if (e != cudaSuccess) fail(NSX_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_y): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[device] = static_cast<double *>(p);
+  }
+  return g_noalloc_ptr[device];
+}
+
+int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
+
+}  // namespace nsx
+
+int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream) {
+  if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
+  if (x == y) fail(NSX_E_ARG, "x and y must not alias");
+  if (h->y_elems > NOALLOC_Y_MAX)
+    fail(NSX_E_ARG, "problem needs " + std::to_string(h->y_elems) + " FP64 scratch elements; the fixed array of "
+                        "nsx_matvec_noalloc holds " + std::to_string(NOALLOC_Y_MAX) + " (use nsx_matvec)");
+  NSX_CUDA(cudaSetDevice(h->device));
+  double *Y = noalloc_scratch(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  // unreachable column slabs of Y are read as zeros by the proton-side stage
+  if (h->y_elems > 0) NSX_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)h->y_elems, s));
+  matvec_fp64_with_scratch(h, x, y, Y, s);
+  return NSX_OK;
+}

@@ -150,6 +150,7 @@ void upload(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);
+void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *Y, cudaStream_t s);
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]);
 void flush_stage_events(nsx_handle *h);
 double sixj(int a, int b, int c, int d, int e, int f);

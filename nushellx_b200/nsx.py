@@ -84,6 +84,7 @@ SYMBOLS = {
     "nsx_matvec_flops": (C.c_double, [C.c_void_p]),
     "nsx_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
+    "nsx_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
     "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
     "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
@@ -243,6 +244,11 @@ class Solver:
         """Device pointers (e.g. torch tensor .data_ptr()); stream is a cudaStream_t integer or None."""
         _check(self._lib.nsx_matvec(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), precision,
                                     C.c_void_p(stream) if stream else None))
+
+    def matvec_noalloc(self, x_ptr, y_ptr, stream=None):
+        """FP64 H.v with the fixed device scratch array (no allocation in the call)."""
+        _check(self._lib.nsx_matvec_noalloc(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                            C.c_void_p(stream) if stream else None))
 
     def solve(self, nev=10, tol=1e-6, precision=NSX_FP64, window=100, keep=0, max_iter=3000, pre_iter=2,
               seed=5, start=None, refine=False, want_vectors=False):
