@@ -160,17 +160,19 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
               nsx_report *report);
 
 /* Device-side statistics of a handle (for benchmarking and profiling).
- * Stages of one H.v: 0 = like-particle GEMMs (k_like), 1 = neutron-side Y
- * products (k_y), 2 = mixing + proton side (k_a), 3 = precision conversion.
- * With timing enabled every stage launch is bracketed by CUDA events on its
- * stream; nsx_get_stats synchronises and sums them. */
+ * Stages of one H.v: 0 = like-particle products (k_like), 1 = neutron-side Y
+ * products (k_y), 2 = mixing into the stacked operands (k_z), 3 = proton-side
+ * products (k_a), 4 = FP64 <-> FP32 conversions.  With timing enabled every
+ * stage launch is bracketed by CUDA events on its stream; nsx_get_stats
+ * synchronises and sums them. */
+#define NSX_STAGES 5
 typedef struct nsx_stats {
   int64_t launches;           /* kernels launched by the library since the reset   */
   int64_t matvecs;            /* H.v products since the reset                        */
-  int64_t stage_launches[4];
-  double stage_ms[4];         /* summed device time per stage (timing enabled only) */
-  double stage_bytes[4];      /* algorithmic HBM bytes of one launch of each stage  */
-  double stage_flops[4];      /* algorithmic flops of one launch of each stage      */
+  int64_t stage_launches[NSX_STAGES];
+  double stage_ms[NSX_STAGES];     /* summed device time per stage (timing enabled only) */
+  double stage_bytes[NSX_STAGES];  /* algorithmic HBM bytes of one launch of each stage  */
+  double stage_flops[NSX_STAGES];  /* algorithmic flops of one launch of each stage      */
 } nsx_stats;
 
 /* Reset the counters; enable (1) or disable (0) per-stage event timing. */

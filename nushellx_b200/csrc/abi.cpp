@@ -152,7 +152,7 @@ int nsx_stats_reset(nsx_handle *h, int32_t timing) {
     if (!h) fail(NSX_E_ARG, "null handle");
     flush_stage_events(h);
     h->launches = h->matvecs = 0;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < NSX_STAGES; ++i) {
       h->stage_launches[i] = 0;
       h->stage_ms[i] = 0;
     }
@@ -170,7 +170,7 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
     // algorithmic figures for the precision of the last H.v
     int prec = h->last_precision;
     stage_bytes_flops(h, prec, out->stage_bytes, out->stage_flops);
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < NSX_STAGES; ++i) {
       out->stage_launches[i] = h->stage_launches[i];
       out->stage_ms[i] = h->stage_ms[i];
     }

@@ -3,16 +3,20 @@
 // The reference computes the product as multiplyx (pn), multiplya (pp) and
 // multiplyb (nn) in src/NuLnz/NuCoreX.f90:76-226 with axpy loops over density
 // sub-blocks (src/NuCommonX/NuCommonX.f90:745-919, 1009-1104).  Here it is
-// three stream-ordered kernels, each output element owned by exactly one CTA
-// (no atomics, no per-thread vector copies):
+// four stream-ordered kernels; every output element is owned by one thread
+// block (no atomics, no per-thread copies of the vector):
 //
-//   k_like : out_b  = H_pp(Ja) C_b + C_b H_nn(Jb)              (dense tiled GEMM)
+//   k_like : out_b = H_pp(Ja) C_b + C_b H_nn(Jb)                  (dense tiled GEMM)
 //   k_y    : Y_(h,k) = C_h rho_k^T for every (input block h, neutron density k)
-//            that the pn table uses -- computed once and reused by every proton
-//            operator, where the reference recomputes it per proton operator;
-//   k_a    : out[P_l rows] += sum_(a,P_r) rho_a[P_l,P_r] (sum_k w_ak Y_(h,k)[P_r rows])
-//            (mixing of the Y intermediates fused into the operand load).
+//            the pn table uses -- once, where the reference recomputes it for
+//            every proton operator; row-major d_ar x d_bl
+//   k_z    : Z_a[P_r rows] = sum_s w_(a,s) Y_s[P_r rows] for the proton operators
+//            of each (output block, J_ar, lam) group, written as rows of the
+//            stacked operand Zbar of the output slab (block, P_l) a leads to
+//   k_a    : out[P_l rows] += Abar Zbar, Abar = the slab's proton density blocks
+//            side by side: one long-K product per output slab, no mixing
 //
+// Each intermediate (Y, Zbar) is written once and read once, in row streams.
 // Templated on the contraction type: double (the FP64 form) or float (the FP32
 // form, FP64 vectors converted at the boundary).
 #include <algorithm>
@@ -88,6 +92,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
                                            const T *__restrict__ x, const T *__restrict__ rho,
                                            T *__restrict__ Y, int max_nr, int max_nl) {
+  // Y is row-major (ld = g.ldy): thread `row` writes its row's columns of each block
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
   T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
       for (int l = 0; l < b.nl; ++l) {
         T acc = T(0);
         for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
-        Yg[row + (int64_t)g.m * (b.ycol + l)] = acc;
+        Yg[(int64_t)row * g.ldy + (b.ycol + l)] = acc;
       }
     }
     __syncthreads();
@@ -115,77 +120,99 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
 }
 
 // ---------------------------------------------------------------------------
-// k_a: one CTA per output tile (block, P_l, <=64 columns); 256 threads own the
-// nl x ncols outputs (idx = tid + 256 q).  Per contribution: Z = sum w Y rows
-// (mixing) in shared memory, then acc += rho_a Z.
-constexpr int AQ = 16;  // outputs per thread: supports nl <= 64 with 64 columns
-struct KaLayout {  // byte offsets of the k_a shared-memory arrays (16-byte aligned)
-  size_t rs, zs, ws, ys, ls, total;
-  __host__ __device__ static size_t al(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ KaLayout(size_t es, int nl, int nr, int nm) {
-    rs = 0;
-    zs = al(rs + es * (size_t)nl * nr);
-    ws = al(zs + es * (size_t)nr * 64);
-    ys = al(ws + es * (size_t)nm);
-    ls = al(ys + 8 * (size_t)nm);
-    total = al(ls + 4 * (size_t)nm);
-  }
-};
-template <typename T>
-__global__ void __launch_bounds__(256) k_a(const ATile *__restrict__ tiles, const AContrib *__restrict__ contribs,
-                                           const AMix *__restrict__ mixes, const T *__restrict__ wts,
-                                           const T *__restrict__ rho, const T *__restrict__ Y, T *__restrict__ out,
-                                           int max_nr, int max_nl, int max_mix) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  KaLayout L(sizeof(T), max_nl, max_nr, max_mix);
-  T *rs = reinterpret_cast<T *>(smem_raw + L.rs);        // [max_nl*max_nr]
-  T *zs = reinterpret_cast<T *>(smem_raw + L.zs);        // [max_nr][64]
-  T *ws = reinterpret_cast<T *>(smem_raw + L.ws);        // [max_mix]
-  int64_t *ys = reinterpret_cast<int64_t *>(smem_raw + L.ys);  // [max_mix]
-  int *ls = reinterpret_cast<int *>(smem_raw + L.ls);    // [max_mix]
-  const ATile t = tiles[blockIdx.x];
-  const int nl = t.nl, ncols = t.ncols;
-  T acc[AQ];
+// k_z: one CTA per (group, P_r, 128-column tile); thread = column.  For each row
+// of P_r the group's sources are read once into registers and every operator's
+// mixed row is written to its Zbar slab.
+template <typename T, int NS>
+__device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], const int64_t *ysrc, const int64_t *zdst,
+                                        int ns, int na, const T *__restrict__ Y, T *__restrict__ Zb) {
+  const int c = threadIdx.x;
+  if (c >= u.ncols) return;
+  const int col = u.c0 + c;
+  for (int rr = 0; rr < u.nr; ++rr) {
+    const int64_t roff = (int64_t)(u.row0 + rr) * u.d_bl + col;
+    T y[NS];
 #pragma unroll
-  for (int q = 0; q < AQ; ++q) acc[q] = T(0);
-  for (int ci = t.c_begin; ci < t.c_end; ++ci) {
-    const AContrib c = contribs[ci];
-    const int nr = c.nr;
-    const int nm = c.m_end - c.m_begin;
-    for (int e = threadIdx.x; e < nl * nr; e += 256) rs[e] = rho[c.rho + e];
-    for (int e = threadIdx.x; e < nm; e += 256) {
-      const AMix m = mixes[c.m_begin + e];
-      ws[e] = wts[m.wi];
-      ys[e] = m.y;
-      ls[e] = m.ld;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < nr * ncols; e += 256) {
-      const int k = e % nr, j = e / nr;
+    for (int s = 0; s < NS; ++s) y[s] = s < ns ? Y[ysrc[s] + roff] : T(0);
+    for (int a = 0; a < na; ++a) {
       T z = T(0);
-      for (int m = 0; m < nm; ++m) z = fma(ws[m], Y[ys[m] + k + (int64_t)ls[m] * (t.col0 + j)], z);
-      zs[k * 64 + j] = z;
-    }
-    __syncthreads();
 #pragma unroll
-    for (int q = 0; q < AQ; ++q) {
-      const int idx = threadIdx.x + 256 * q;
-      const int i = idx % nl, j = idx / nl;
-      if (j < ncols) {
-        T a = acc[q];
-        for (int k = 0; k < nr; ++k) a = fma(rs[i + nl * k], zs[k * 64 + j], a);
-        acc[q] = a;
+      for (int s = 0; s < NS; ++s) z = fma(ws[a][s], y[s], z);
+      Zb[zdst[a] + (int64_t)rr * u.d_bl + col] = z;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, const ZGroup *__restrict__ groups,
+                                           const ZSrc *__restrict__ srcs, const ZOp *__restrict__ ops,
+                                           const T *__restrict__ W, const T *__restrict__ Y, T *__restrict__ Zb) {
+  __shared__ T ws[ZMAXA][ZMAXS];
+  __shared__ int64_t ysrc[ZMAXS];
+  __shared__ int64_t zdst[ZMAXA];
+  const ZUnit u = units[blockIdx.x];
+  const ZGroup G = groups[u.grp];
+  const int na = u.op_end - u.op_begin;
+  for (int e = threadIdx.x; e < na * ZMAXS; e += blockDim.x) {
+    const int a = e / ZMAXS, s = e - a * ZMAXS;
+    ws[a][s] = s < G.ns ? W[G.w_off + ops[u.op_begin + a].wrow * G.ns + s] : T(0);
+  }
+  for (int e = threadIdx.x; e < na; e += blockDim.x) zdst[e] = ops[u.op_begin + e].z;
+  for (int e = threadIdx.x; e < ZMAXS; e += blockDim.x) ysrc[e] = e < G.ns ? srcs[G.s_begin + e].y : 0;
+  __syncthreads();
+  if (G.ns <= 16)
+    kz_body<T, 16>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
+  else
+    kz_body<T, 32>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
+}
+
+// ---------------------------------------------------------------------------
+// k_a: one CTA per (output slab P_l, 128-column tile); 256 threads = 4 row
+// slots x 64 column pairs, rows l = slot + 4j (nl <= 64).  Abar is staged in
+// shared memory in chunks of KC stacked rows; each thread streams its two
+// Zbar columns.
+constexpr int KA_KC = 128;
+template <typename T>
+__global__ void __launch_bounds__(256) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
+                                           const T *__restrict__ Zb, T *__restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *as = reinterpret_cast<T *>(smem_raw);  // [KC][nl]
+  const ATile t = tiles[blockIdx.x];
+  const int nl = t.nl;
+  const int rs = threadIdx.x / 64, cp = threadIdx.x % 64;
+  const int c0 = 2 * cp, c1 = 2 * cp + 1;
+  T acc0[16], acc1[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc0[j] = acc1[j] = T(0);
+  const T *Z = Zb + t.zbar;
+  for (int k0 = 0; k0 < t.K; k0 += KA_KC) {
+    const int kc = min(KA_KC, t.K - k0);
+    const T *Ak = Abar + t.abar + (int64_t)k0 * nl;
+    for (int e = threadIdx.x; e < kc * nl; e += blockDim.x) as[e] = Ak[e];
+    __syncthreads();
+    for (int k = 0; k < kc; ++k) {
+      const T *Zr = Z + (int64_t)(k0 + k) * t.ldz;
+      const T z0 = c0 < t.ncols ? Zr[c0] : T(0);
+      const T z1 = c1 < t.ncols ? Zr[c1] : T(0);
+      const T *ak = as + k * nl;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int l = rs + 4 * j;
+        if (l < nl) {
+          const T a = ak[l];
+          acc0[j] = fma(a, z0, acc0[j]);
+          acc1[j] = fma(a, z1, acc1[j]);
+        }
       }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int q = 0; q < AQ; ++q) {
-    const int idx = threadIdx.x + 256 * q;
-    const int i = idx % nl, j = idx / nl;
-    if (j < ncols) {
-      T *o = out + t.out + i + (int64_t)t.ld * j;
-      *o += acc[q];
+  for (int j = 0; j < 16; ++j) {
+    const int l = rs + 4 * j;
+    if (l < nl) {
+      if (c0 < t.ncols) out[t.out + l + (int64_t)t.ld * c0] += acc0[j];
+      if (c1 < t.ncols) out[t.out + l + (int64_t)t.ld * c1] += acc1[j];
     }
   }
 }
@@ -223,24 +250,25 @@ static S *dev_copy_pod(const std::vector<S> &v) {
 static size_t ky_smem(const nsx_handle *h, size_t es) {
   return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
 }
-static size_t ka_smem(const nsx_handle *h, size_t es) {
-  return KaLayout(es, h->max_anl, h->max_anr, h->max_mix).total;
-}
+static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
-  if (h->max_anl > AQ * 256 / 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
+  if (h->max_anl > 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
   d.rhoA = dev_copy<double>(h->A.vals);
   d.rhoB = dev_copy<double>(h->B.vals);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
   d.w = dev_copy<double>(h->weights);
+  d.abar = dev_copy<double>(h->abar);
   d.ygroups = dev_copy_pod(h->ygroups);
   d.yblks = dev_copy_pod(h->yblks);
+  d.zgroups = dev_copy_pod(h->zgroups);
+  d.zsrcs = dev_copy_pod(h->zsrcs);
+  d.zunits = dev_copy_pod(h->zunits);
+  d.zops = dev_copy_pod(h->zops);
   d.atiles = dev_copy_pod(h->atiles);
-  d.acontribs = dev_copy_pod(h->acontribs);
-  d.amixes = dev_copy_pod(h->amixes);
   d.ltiles = dev_copy_pod(h->ltiles);
   NSX_CUDA(cudaMalloc(&d.xin, h->no_state * sizeof(double)));
   NSX_CUDA(cudaMalloc(&d.xout, h->no_state * sizeof(double)));
@@ -258,21 +286,24 @@ void upload(nsx_handle *h) {
 
 void ensure_precision(nsx_handle *h, int precision) {
   auto &d = h->d;
-  size_t ny = std::max<int64_t>(h->y_elems, 1);
+  size_t ny = std::max<int64_t>(h->y_elems, 1), nz = std::max<int64_t>(h->z_elems, 1);
   if (precision == NSX_FP64) {
     if (!d.y64) {
       NSX_CUDA(cudaMalloc(&d.y64, ny * sizeof(double)));
       NSX_CUDA(cudaMemset(d.y64, 0, ny * sizeof(double)));  // unreachable column slabs stay zero
+      NSX_CUDA(cudaMalloc(&d.z64, nz * sizeof(double)));
     }
   } else if (precision == NSX_FP32) {
     if (!d.y32) {
       NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
       NSX_CUDA(cudaMemset(d.y32, 0, ny * sizeof(float)));
+      NSX_CUDA(cudaMalloc(&d.z32, nz * sizeof(float)));
       d.rhoA32 = dev_copy<float>(h->A.vals);
       d.rhoB32 = dev_copy<float>(h->B.vals);
       d.hA32 = dev_copy<float>(h->A.hdense);
       d.hB32 = dev_copy<float>(h->B.hdense);
       d.w32 = dev_copy<float>(h->weights);
+      d.abar32 = dev_copy<float>(h->abar);
       NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
     }
@@ -318,25 +349,29 @@ void flush_stage_events(nsx_handle *h) {
 
 // Algorithmic traffic (each operand read once, each result written once) and
 // flops of one launch of each stage.
-void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]) {
+void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]) {
   const double es = precision == NSX_FP64 ? 8.0 : 4.0;
   const double n = (double)h->no_state;
   double rhoA = (double)h->A.vals.size(), rhoB = (double)h->B.vals.size();
   double hd = (double)(h->A.hdense.size() + h->B.hdense.size());
-  bytes[0] = es * (2.0 * n + hd);                               // C in, out written, dense H
-  bytes[1] = es * (n + rhoB + (double)h->y_elems);              // C in, rho_B, Y written
-  bytes[2] = es * ((double)h->y_elems + rhoA + 2.0 * n) + 4.0 * (double)h->weights.size();  // Y, rho_A, out r/w
-  bytes[3] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);     // one conversion launch
+  const double y = (double)h->y_elems, z = (double)h->z_elems;
+  bytes[0] = es * (2.0 * n + hd);                         // C in, out written, dense H
+  bytes[1] = es * (n + rhoB + y);                         // C in, rho_B, Y written
+  bytes[2] = es * (y + z + (double)h->weights.size());    // Y in, Zbar written
+  bytes[3] = es * (z + (double)h->abar.size() + 2.0 * n); // Zbar in, Abar, out read + written
+  bytes[4] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);
   flops[0] = h->flops_like;
   flops[1] = h->flops_y;
-  flops[2] = h->flops_mix + h->flops_a;
-  flops[3] = 0.0;
+  flops[2] = h->flops_mix;
+  flops[3] = h->flops_a;
+  flops[4] = 0.0;
 }
 
 template <typename T>
 static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T *rhoB, const T *hA, const T *hB,
-                       const T *w, T *Y, cudaStream_t s) {
+                       const T *w, const T *abar, T *Y, T *Z, cudaStream_t s) {
   auto &d = h->d;
+  (void)rhoA;
   if (!h->ltiles.empty()) {
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
@@ -346,10 +381,13 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
     k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
                                                                              h->max_ynr, h->max_ynl);
   }
-  if (!h->atiles.empty()) {
+  if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);
-    k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(
-        d.atiles, d.acontribs, d.amixes, w, rhoA, Y, out, h->max_anr, h->max_anl, h->max_mix);
+    k_z<T><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
+  }
+  if (!h->atiles.empty()) {
+    StageScope sc(h, 3, s);
+    k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(d.atiles, abar, Z, out);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -360,35 +398,37 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   h->matvecs++;
   h->last_precision = precision;
   if (precision == NSX_FP64) {
-    run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.y64, s);
+    run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, d.y64, d.z64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
     {
-      StageScope sc(h, 3, s);
+      StageScope sc(h, 4, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.y32, s);
+    run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32, d.y32, d.z32, s);
     {
-      StageScope sc(h, 3, s);
+      StageScope sc(h, 4, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
     }
     NSX_CUDA(cudaGetLastError());
   }
 }
 
-// The FP64 stages with a caller-provided Y buffer (used by the fixed-scratch entry point).
-void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *Y, cudaStream_t s) {
+// The FP64 stages with a caller-provided scratch buffer: Y (y_elems, zero where no
+// density block reaches) followed by Zbar (z_elems).  Used by the fixed-scratch entry point.
+void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s) {
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = NSX_FP64;
-  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, Y, s);
+  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + h->y_elems, s);
 }
 
 void release(nsx_handle *h) {
   auto &d = h->d;
-  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.ygroups, d.yblks,
-                  d.atiles, d.acontribs, d.amixes, d.ltiles, d.y64, d.y32, d.x32, d.o32, d.xin, d.xout};
+  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
+                  d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zops, d.atiles, d.ltiles,
+                  d.y64, d.z64, d.y32, d.z32, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceBuffers();

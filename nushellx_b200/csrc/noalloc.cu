@@ -8,8 +8,9 @@
 // scratch is the file-scope array below, of a fixed maximum size.
 //
 // Rules for callers:
-// * The array holds NOALLOC_Y_MAX FP64 elements (64 MiB); a problem whose Y
-//   intermediates need more is rejected with NSX_E_ARG and a message.
+// * The array holds NOALLOC_Y_MAX FP64 elements (64 MiB); a problem whose
+//   intermediates (Y and the stacked Zbar) need more is rejected with NSX_E_ARG
+//   and a message.
 // * The first call on a device looks up the array's device address (this
 //   loads the library's module on that device if it is not loaded yet); make
 //   that first call before any stream capture.  Every GPU that loads the
@@ -51,13 +52,14 @@ int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream) {
   if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
   if (x == y) fail(NSX_E_ARG, "x and y must not alias");
-  if (h->y_elems > NOALLOC_Y_MAX)
-    fail(NSX_E_ARG, "problem needs " + std::to_string(h->y_elems) + " FP64 scratch elements; the fixed array of "
+  const int64_t need = h->y_elems + h->z_elems;
+  if (need > NOALLOC_Y_MAX)
+    fail(NSX_E_ARG, "problem needs " + std::to_string(need) + " FP64 scratch elements; the fixed array of "
                         "nsx_matvec_noalloc holds " + std::to_string(NOALLOC_Y_MAX) + " (use nsx_matvec)");
   NSX_CUDA(cudaSetDevice(h->device));
   double *Y = noalloc_scratch(h->device);
   cudaStream_t s = (cudaStream_t)stream;
-  // unreachable column slabs of Y are read as zeros by the proton-side stage
+  // the array holds Y then Zbar; column slabs of Y that no density block reaches are read as zeros
   if (h->y_elems > 0) NSX_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)h->y_elems, s));
   matvec_fp64_with_scratch(h, x, y, Y, s);
   return NSX_OK;

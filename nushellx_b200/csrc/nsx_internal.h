@@ -54,13 +54,15 @@ struct Block {
 };
 
 // ---- task lists of the H.v kernels -------------------------------------------
-// Y stage: Y_(h,b) = C_h * rho_b^T, one group per (Y matrix, row tile).
+// Y stage: Y_(h,b) = C_h * rho_b^T (row-major d_ar x d_bl), one group per (Y matrix, row tile).
 struct YGroup {
   int64_t c_base;   // element offset of input block h
-  int64_t y_base;   // element offset of the Y matrix (d_ar x d_bl, column-major)
-  int32_t m;        // d_ar (rows, leading dimension of C_h and Y)
+  int64_t y_base;   // element offset of the Y matrix
+  int32_t m;        // d_ar (rows; leading dimension of C_h)
   int32_t row0;     // first row of the tile
   int32_t b_begin, b_end;  // range in yblks
+  int32_t ldy;      // d_bl (row length of Y)
+  int32_t pad;
 };
 struct YBlk {
   int64_t rho;      // offset of the nl x nr (column-major) density sub-block
@@ -68,23 +70,41 @@ struct YBlk {
   int32_t ycol;     // first column of Y (left partition Q_l)
   int32_t nl, nr;
 };
-// A stage: output tile (block, left proton partition P_l, column range).
+// Mixing stage k_z: Z_a[P_r rows] = sum_s w_(a,s) Y_s[P_r rows] for the proton operators a of a
+// group (output block, J_ar, lam) acting on P_r; written into the stacked operand Zbar.
+constexpr int ZMAXS = 32;   // sources (h, b) per group
+constexpr int ZMAXA = 16;   // proton operators per group
+struct ZGroup {
+  int32_t s_begin, s_end;   // range in zsrcs
+  int32_t ns;               // sources
+  int32_t w_off;            // weights [operator][ns] row-major
+};
+struct ZSrc {
+  int64_t y;                // offset of the source's Y matrix
+};
+struct ZUnit {              // (group, P_r, column tile)
+  int32_t grp;
+  int32_t row0, nr;         // rows of P_r in the J_ar space
+  int32_t c0, ncols;        // column tile
+  int32_t d_bl;             // row length of Y and Zbar
+  int32_t op_begin, op_end; // range in zops
+};
+struct ZOp {
+  int64_t z;                // Zbar destination of the operator: element (row rr of P_r, col c) at z + rr*d_bl + c
+  int32_t wrow;             // weight row within the group
+  int32_t pad;
+};
+// Proton side k_a: out[P_l rows, cols] += Abar (nl x K, column-major) * Zbar (K x d_bl, row-major).
+constexpr int KA_TILE_COLS = 128;   // output columns per k_a tile (64 threads x 2 columns)
 struct ATile {
-  int64_t out;      // element offset of out[P_l row 0, col0] in the output vector
+  int64_t out;      // element offset of out[P_l row 0, col0]
   int32_t ld;       // d_al (leading dimension of the output block)
-  int32_t nl;       // rows of the tile = nJT(P_l, J_al)
+  int32_t nl;       // rows = nJT(P_l, J_al)
   int32_t col0, ncols;
-  int32_t c_begin, c_end;  // range in contribs
-};
-struct AContrib {
-  int64_t rho;      // offset of the nl x nr proton density sub-block (column-major)
-  int32_t nr;       // nJT(P_r, J_ar)
-  int32_t m_begin, m_end;  // range in mixes
-};
-struct AMix {
-  int64_t y;        // offset of Y_(h,b)[P_r row 0, col 0]
-  int32_t ld;       // d_ar (leading dimension of that Y matrix)
-  int32_t wi;       // index into the weight array
+  int32_t ldz;      // d_bl
+  int32_t K;        // stacked contribution rows
+  int64_t zbar;     // offset of Zbar[0, col0]
+  int64_t abar;     // offset of Abar[0, 0]
 };
 // like-particle part: out_blk = Ha C + C Hb, 64x64 output tiles.
 struct LTile {
@@ -98,14 +118,18 @@ struct DeviceBuffers {
   // FP64 operator data
   double *rhoA = nullptr, *rhoB = nullptr, *hA = nullptr, *hB = nullptr, *w = nullptr;
   float *rhoA32 = nullptr, *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr, *w32 = nullptr;
+  double *abar = nullptr;
+  float *abar32 = nullptr;
   YGroup *ygroups = nullptr;
   YBlk *yblks = nullptr;
+  ZGroup *zgroups = nullptr;
+  ZSrc *zsrcs = nullptr;
+  ZUnit *zunits = nullptr;
+  ZOp *zops = nullptr;
   ATile *atiles = nullptr;
-  AContrib *acontribs = nullptr;
-  AMix *amixes = nullptr;
   LTile *ltiles = nullptr;
-  double *y64 = nullptr;   // Y intermediates, FP64
-  float *y32 = nullptr;    // Y intermediates, FP32
+  double *y64 = nullptr, *z64 = nullptr;  // Y and Zbar intermediates, FP64
+  float *y32 = nullptr, *z32 = nullptr;   // Y and Zbar intermediates, FP32
   float *x32 = nullptr, *o32 = nullptr;
   double *xin = nullptr, *xout = nullptr;  // host-API staging
 };
@@ -125,20 +149,23 @@ struct nsx_handle {
   // plan
   std::vector<nsx::YGroup> ygroups;
   std::vector<nsx::YBlk> yblks;
+  std::vector<nsx::ZGroup> zgroups;
+  std::vector<nsx::ZSrc> zsrcs;
+  std::vector<nsx::ZUnit> zunits;
+  std::vector<nsx::ZOp> zops;
   std::vector<nsx::ATile> atiles;
-  std::vector<nsx::AContrib> acontribs;
-  std::vector<nsx::AMix> amixes;
+  std::vector<double> abar;
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
-  int64_t y_elems = 0;
-  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_anr = 0, max_mix = 0;
+  int64_t y_elems = 0, z_elems = 0;
+  int max_ynl = 0, max_ynr = 0, max_anl = 0;
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // statistics
   int64_t launches = 0, matvecs = 0;
-  int64_t stage_launches[4] = {0, 0, 0, 0};
-  double stage_ms[4] = {0, 0, 0, 0};
+  int64_t stage_launches[NSX_STAGES] = {};
+  double stage_ms[NSX_STAGES] = {};
   bool timing = false;
   int last_precision = NSX_FP64;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
@@ -150,8 +177,8 @@ void upload(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);
-void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *Y, cudaStream_t s);
-void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[4], double flops[4]);
+void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s);
+void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]);
 void flush_stage_events(nsx_handle *h);
 double sixj(int a, int b, int c, int d, int e, int f);
 double racah_w(int j1, int j2, int j3, int j4, int J, int K);

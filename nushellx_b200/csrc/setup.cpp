@@ -213,44 +213,21 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   }
 
   // ---- pn table (drdbh, src/NuLnz/NuCoreX.f90:1428-1577) ----------------------
-  // entries per (output block, J_ar, a-key): list of (b-key, input block, weight)
+  // Rows: (output block, J_ar, proton density key a) with entries (neutron key b, input block h, weight).
   struct Entry { int bk, hb; double w; };
-  std::map<std::pair<int, int>, int> ymat;  // (input block, b-key) -> Y matrix index
-  std::vector<std::pair<int, int>> ymats;
-  std::vector<int64_t> yoff;
-  h->weights.clear();
-  h->ygroups.clear();
-  h->yblks.clear();
-  h->atiles.clear();
-  h->acontribs.clear();
-  h->amixes.clear();
-  h->flops_y = h->flops_mix = h->flops_a = 0;
-  int64_t ytot = 0;
-  auto get_ymat = [&](int hb, int bk) {
-    auto it = ymat.find({hb, bk});
-    if (it != ymat.end()) return it->second;
-    int id = (int)ymats.size();
-    ymat[{hb, bk}] = id;
-    ymats.push_back({hb, bk});
-    yoff.push_back(ytot);
-    int J2bl = (int)(B.keys[bk] & 255);
-    ytot += (int64_t)h->blocks[hb].da * B.dim(J2bl);
-    return id;
-  };
-  const int TW = 64;  // output columns per k_a tile
+  struct Row { int bl, jar, ak, lam; std::vector<Entry> e; };
+  std::vector<Row> table;
   for (size_t bl = 0; bl < h->blocks.size(); ++bl) {
     const Block &ob = h->blocks[bl];
     if (ob.da == 0 || ob.db == 0) continue;
-    // contributions per left partition P_l
-    std::vector<std::vector<AContrib>> per_pl(A.nspart);
-    std::vector<std::vector<std::vector<AMix>>> per_pl_mix(A.nspart);
     for (int jar = A.minJ2; jar <= A.maxJ2; jar += 2) {
       auto ait = akeys.find({ob.J2a, jar});
       if (ait == akeys.end()) continue;
       for (int ak : ait->second) {
+        if (A.kblocks[ak].empty()) continue;
         uint64_t akey = A.keys[ak];
         int sal = (akey >> 16) & 255, sar = (akey >> 24) & 255, lam = (akey >> 32) & 255;
-        std::vector<Entry> ents;
+        Row row{(int)bl, jar, ak, lam, {}};
         int jbrn = std::max(std::abs(ob.J2b - lam), std::abs(jar - J2));
         int jbrx = std::min(std::min(ob.J2b + lam, jar + J2), B.maxJ2);
         for (int jbr = jbrn; jbr <= jbrx; jbr += 2) {
@@ -269,65 +246,33 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
             auto vit = h->vop.find(pack_key(sal, sar, sbl, sbr, lam));
             if (vit == h->vop.end() || vit->second == 0.0) continue;
             if (B.kblocks[bk].empty()) continue;
-            ents.push_back({bk, hit->second, vit->second * rw});
+            row.e.push_back({bk, hit->second, vit->second * rw});
           }
         }
-        if (ents.empty() || A.kblocks[ak].empty()) continue;
-        for (const RhoBlk &rb : A.kblocks[ak]) {
-          if (rb.pl >= A.nspart) continue;
-          int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
-          AContrib c;
-          c.rho = rb.voff;
-          c.nr = nr;
-          std::vector<AMix> mx;
-          for (const Entry &e : ents) {
-            int yid = get_ymat(e.hb, e.bk);
-            AMix m;
-            m.y = yoff[yid] + A.poff[A.jidx(jar)][rb.pr];
-            m.ld = h->blocks[e.hb].da;
-            m.wi = (int)h->weights.size();
-            h->weights.push_back(e.w);
-            mx.push_back(m);
-          }
-          per_pl[rb.pl].push_back(c);
-          per_pl_mix[rb.pl].push_back(std::move(mx));
-          h->flops_a += 2.0 * nl * nr * ob.db;
-          h->flops_mix += 2.0 * nr * ob.db * ents.size();
-        }
+        if (!row.e.empty()) table.push_back(std::move(row));
       }
     }
-    std::vector<ATile> btiles;  // this output block's tiles, reordered below
-    for (int pl = 0; pl < A.nspart; ++pl) {
-      int nl = A.njt_of(pl, ob.J2a);
-      if (nl == 0 || per_pl[pl].empty()) continue;
-      int cb = (int)h->acontribs.size();
-      for (size_t i = 0; i < per_pl[pl].size(); ++i) {
-        AContrib c = per_pl[pl][i];
-        c.m_begin = (int)h->amixes.size();
-        for (auto &m : per_pl_mix[pl][i]) h->amixes.push_back(m);
-        c.m_end = (int)h->amixes.size();
-        h->acontribs.push_back(c);
-      }
-      int ce = (int)h->acontribs.size();
-      for (int c0 = 0; c0 < ob.db; c0 += TW) {
-        ATile t;
-        t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
-        t.ld = ob.da;
-        t.nl = nl;
-        t.col0 = c0;
-        t.ncols = std::min(TW, ob.db - c0);
-        t.c_begin = cb;
-        t.c_end = ce;
-        btiles.push_back(t);
-      }
-    }
-    // Tiles of the same column range are launched next to each other: they mix the same
-    // Y column slabs (all proton rows P_r) in the same contribution order, so their reads
-    // meet in L2 instead of each going to DRAM.
-    std::stable_sort(btiles.begin(), btiles.end(), [](const ATile &x, const ATile &y) { return x.col0 < y.col0; });
-    h->atiles.insert(h->atiles.end(), btiles.begin(), btiles.end());
   }
-  // Y groups: one per (Y matrix, 128-row tile), sharing the matrix's sub-block list
+  // ---- Y operands: one row-major d_ar x d_bl matrix per (input block h, neutron key b) ----
+  std::map<std::pair<int, int>, int> ymat;
+  std::vector<std::pair<int, int>> ymats;
+  std::vector<int64_t> yoff;
+  int64_t ytot = 0;
+  auto get_ymat = [&](int hb, int bk) {
+    auto it = ymat.find({hb, bk});
+    if (it != ymat.end()) return it->second;
+    int id = (int)ymats.size();
+    ymat[{hb, bk}] = id;
+    ymats.push_back({hb, bk});
+    yoff.push_back(ytot);
+    ytot += (int64_t)h->blocks[hb].da * B.dim((int)(B.keys[bk] & 255));
+    return id;
+  };
+  for (const Row &r : table)
+    for (const Entry &e : r.e) get_ymat(e.hb, e.bk);
+  h->ygroups.clear();
+  h->yblks.clear();
+  h->flops_y = 0;
   for (size_t y = 0; y < ymats.size(); ++y) {
     int hb = ymats[y].first, bk = ymats[y].second;
     const Block &ib = h->blocks[hb];
@@ -346,19 +291,145 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     }
     int b1 = (int)h->yblks.size();
     h->flops_y += 2.0 * ib.da * nnz;
-    for (int r0 = 0; r0 < ib.da; r0 += 128) h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1});
+    for (int r0 = 0; r0 < ib.da; r0 += 128)
+      h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), 0});
   }
+  // ---- stacked proton side: per output (block, P_l) the contributions (a, P_r) in a fixed
+  // order; Abar = their density blocks side by side (nl x K column-major), Zbar = K x d_bl
+  // row-major mixed operands written by k_z and consumed by k_a ----
+  h->weights.clear();
+  h->zgroups.clear();
+  h->zsrcs.clear();
+  h->zunits.clear();
+  h->zops.clear();
+  h->atiles.clear();
+  h->abar.clear();
+  h->flops_mix = h->flops_a = 0;
+  std::map<std::pair<int, int>, int> slab;  // (block, P_l) -> slab index
+  std::vector<std::pair<int, int>> slabs;
+  std::vector<int> slabK;
+  std::vector<std::vector<std::pair<int, int64_t>>> slab_blocks;  // (nr, rho offset) in K order
+  auto get_slab = [&](int bl, int pl) {
+    auto it = slab.find({bl, pl});
+    if (it != slab.end()) return it->second;
+    int id = (int)slabs.size();
+    slab[{bl, pl}] = id;
+    slabs.push_back({bl, pl});
+    slabK.push_back(0);
+    slab_blocks.push_back({});
+    return id;
+  };
+  // groups: (block, J_ar, lam) -> table rows
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  for (size_t i = 0; i < table.size(); ++i) groups[{table[i].bl, table[i].jar, table[i].lam}].push_back((int)i);
+  struct PendingOp { int slab, kofs, wrow; };
+  struct Pending { int gid, row0, nr; std::vector<PendingOp> ops; };
+  std::vector<Pending> pending;  // one per (group, right proton partition P_r)
+  for (auto &gk : groups) {
+    const int bl = std::get<0>(gk.first), jar = std::get<1>(gk.first);
+    const Block &ob = h->blocks[bl];
+    const std::vector<int> &rows = gk.second;
+    std::map<std::pair<int, int>, int> sidx;
+    std::vector<std::pair<int, int>> srcs;
+    for (int r : rows)
+      for (const Entry &e : table[r].e)
+        if (!sidx.count({e.hb, e.bk})) {
+          sidx[{e.hb, e.bk}] = (int)srcs.size();
+          srcs.push_back({e.hb, e.bk});
+        }
+    if (srcs.size() > (size_t)ZMAXS || rows.size() > (size_t)ZMAXA)
+      fail(NSX_E_ARG, "pn group exceeds the mixing limits (sources or proton operators)");
+    ZGroup G;
+    G.s_begin = (int)h->zsrcs.size();
+    for (auto &sr : srcs) h->zsrcs.push_back({yoff[get_ymat(sr.first, sr.second)]});
+    G.s_end = (int)h->zsrcs.size();
+    G.ns = (int)srcs.size();
+    G.w_off = (int)h->weights.size();
+    for (int r : rows) {
+      std::vector<double> wr(G.ns, 0.0);
+      for (const Entry &e : table[r].e) wr[sidx[{e.hb, e.bk}]] += e.w;
+      h->weights.insert(h->weights.end(), wr.begin(), wr.end());
+    }
+    const int gid = (int)h->zgroups.size();
+    h->zgroups.push_back(G);
+    // operators per right proton partition
+    std::map<int, std::vector<PendingOp>> by_pr;
+    for (size_t ai = 0; ai < rows.size(); ++ai) {
+      const Row &r = table[rows[ai]];
+      for (const RhoBlk &rb : A.kblocks[r.ak]) {
+        int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
+        int sl = get_slab(bl, rb.pl);
+        PendingOp op{sl, slabK[sl], (int)ai};
+        slabK[sl] += nr;
+        slab_blocks[sl].push_back({nr, rb.voff});
+        by_pr[rb.pr].push_back(op);
+        h->flops_a += 2.0 * nl * nr * ob.db;
+        h->flops_mix += 2.0 * nr * ob.db * G.ns;
+      }
+    }
+    for (auto &pp : by_pr) pending.push_back({gid, A.poff[A.jidx(jar)][pp.first], A.njt_of(pp.first, jar), pp.second});
+  }
+  // Zbar slabs and Abar
+  std::vector<int64_t> zoff(slabs.size());
+  int64_t ztot = 0;
+  for (size_t sl = 0; sl < slabs.size(); ++sl) {
+    zoff[sl] = ztot;
+    ztot += (int64_t)slabK[sl] * h->blocks[slabs[sl].first].db;
+  }
+  // k_z units: (group, P_r, 128-column tile)
+  const int ZT = 128;
+  for (auto &pd : pending) {
+    const int bl = slabs[pd.ops[0].slab].first;
+    const Block &ob = h->blocks[bl];
+    if (pd.ops.size() > (size_t)ZMAXA) fail(NSX_E_ARG, "too many proton operators on one partition");
+    int op0 = (int)h->zops.size();
+    for (const PendingOp &o : pd.ops) h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ob.db, o.wrow, 0});
+    int op1 = (int)h->zops.size();
+    for (int c0 = 0; c0 < ob.db; c0 += ZT) {
+      ZUnit u;
+      u.grp = pd.gid;
+      u.row0 = pd.row0;
+      u.nr = pd.nr;
+      u.c0 = c0;
+      u.ncols = std::min(ZT, ob.db - c0);
+      u.d_bl = ob.db;
+      u.op_begin = op0;
+      u.op_end = op1;
+      h->zunits.push_back(u);
+    }
+  }
+  // k_a tiles: (slab, KA_TILE_COLS-column tile)
+  const int TW = KA_TILE_COLS;
+  for (size_t sl = 0; sl < slabs.size(); ++sl) {
+    const int bl = slabs[sl].first, pl = slabs[sl].second;
+    const Block &ob = h->blocks[bl];
+    int64_t a0 = (int64_t)h->abar.size();
+    for (auto &bv : slab_blocks[sl]) {
+      int nl = A.njt_of(pl, ob.J2a);
+      h->abar.insert(h->abar.end(), A.vals.begin() + bv.second, A.vals.begin() + bv.second + (int64_t)nl * bv.first);
+    }
+    for (int c0 = 0; c0 < ob.db; c0 += TW) {
+      ATile t;
+      t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
+      t.ld = ob.da;
+      t.nl = A.njt_of(pl, ob.J2a);
+      t.col0 = c0;
+      t.ncols = std::min(TW, ob.db - c0);
+      t.ldz = ob.db;
+      t.zbar = zoff[sl] + c0;
+      t.abar = a0;
+      t.K = slabK[sl];
+      h->atiles.push_back(t);
+    }
+  }
+  h->z_elems = ztot;
   h->y_elems = ytot;
-  h->max_ynl = h->max_ynr = h->max_anl = h->max_anr = h->max_mix = 0;
+  h->max_ynl = h->max_ynr = h->max_anl = 0;
   for (auto &y : h->yblks) {
     h->max_ynl = std::max(h->max_ynl, y.nl);
     h->max_ynr = std::max(h->max_ynr, y.nr);
   }
   for (auto &t : h->atiles) h->max_anl = std::max(h->max_anl, t.nl);
-  for (auto &c : h->acontribs) {
-    h->max_anr = std::max(h->max_anr, c.nr);
-    h->max_mix = std::max(h->max_mix, c.m_end - c.m_begin);
-  }
 }
 
 }  // namespace nsx

@@ -54,10 +54,10 @@ class Report(C.Structure):
 
 
 class Stats(C.Structure):
-    _fields_ = [("launches", C.c_int64), ("matvecs", C.c_int64), ("stage_launches", C.c_int64 * 4),
-                ("stage_ms", C.c_double * 4), ("stage_bytes", C.c_double * 4), ("stage_flops", C.c_double * 4)]
+    _fields_ = [("launches", C.c_int64), ("matvecs", C.c_int64), ("stage_launches", C.c_int64 * 5),
+                ("stage_ms", C.c_double * 5), ("stage_bytes", C.c_double * 5), ("stage_flops", C.c_double * 5)]
 
-    STAGES = ("k_like", "k_y", "k_a", "k_convert")
+    STAGES = ("k_like", "k_y", "k_z", "k_a", "k_convert")
 
     def as_dict(self):
         return {"launches": self.launches, "matvecs": self.matvecs,
