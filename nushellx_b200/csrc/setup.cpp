@@ -337,37 +337,53 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           sidx[{e.hb, e.bk}] = (int)srcs.size();
           srcs.push_back({e.hb, e.bk});
         }
-    if (srcs.size() > (size_t)ZMAXS || rows.size() > (size_t)ZMAXA)
-      fail(NSX_E_ARG, "pn group exceeds the mixing limits (sources or proton operators)");
-    ZGroup G;
-    G.s_begin = (int)h->zsrcs.size();
-    for (auto &sr : srcs) h->zsrcs.push_back({yoff[get_ymat(sr.first, sr.second)]});
-    G.s_end = (int)h->zsrcs.size();
-    G.ns = (int)srcs.size();
-    G.w_off = (int)h->weights.size();
-    for (int r : rows) {
-      std::vector<double> wr(G.ns, 0.0);
-      for (const Entry &e : table[r].e) wr[sidx[{e.hb, e.bk}]] += e.w;
-      h->weights.insert(h->weights.end(), wr.begin(), wr.end());
-    }
-    const int gid = (int)h->zgroups.size();
-    h->zgroups.push_back(G);
-    // operators per right proton partition
-    std::map<int, std::vector<PendingOp>> by_pr;
-    for (size_t ai = 0; ai < rows.size(); ++ai) {
-      const Row &r = table[rows[ai]];
-      for (const RhoBlk &rb : A.kblocks[r.ak]) {
-        int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
-        int sl = get_slab(bl, rb.pl);
-        PendingOp op{sl, slabK[sl], (int)ai};
-        slabK[sl] += nr;
-        slab_blocks[sl].push_back({nr, rb.voff});
-        by_pr[rb.pr].push_back(op);
-        h->flops_a += 2.0 * nl * nr * ob.db;
-        h->flops_mix += 2.0 * nr * ob.db * G.ns;
+    // sub-groups of at most ZMAXS sources; each has its own stacked rows (the proton density
+    // block is repeated in Abar), so no two k_z units write the same Zbar row
+    for (size_t s0 = 0; s0 < srcs.size(); s0 += ZMAXS) {
+      const size_t s1 = std::min(srcs.size(), s0 + (size_t)ZMAXS);
+      ZGroup G;
+      G.s_begin = (int)h->zsrcs.size();
+      for (size_t si = s0; si < s1; ++si) h->zsrcs.push_back({yoff[get_ymat(srcs[si].first, srcs[si].second)]});
+      G.s_end = (int)h->zsrcs.size();
+      G.ns = (int)(s1 - s0);
+      G.w_off = (int)h->weights.size();
+      std::vector<char> active(rows.size(), 0);  // operators with a source in this sub-group
+      for (size_t ai = 0; ai < rows.size(); ++ai) {
+        std::vector<double> wr(G.ns, 0.0);
+        for (const Entry &e : table[rows[ai]].e) {
+          int si = sidx[{e.hb, e.bk}];
+          if (si >= (int)s0 && si < (int)s1) {
+            wr[si - s0] += e.w;
+            active[ai] = 1;
+          }
+        }
+        h->weights.insert(h->weights.end(), wr.begin(), wr.end());
       }
+      const int gid = (int)h->zgroups.size();
+      h->zgroups.push_back(G);
+      // operators per right proton partition
+      std::map<int, std::vector<PendingOp>> by_pr;
+      for (size_t ai = 0; ai < rows.size(); ++ai) {
+        if (!active[ai]) continue;
+        const Row &r = table[rows[ai]];
+        for (const RhoBlk &rb : A.kblocks[r.ak]) {
+          int nl = A.njt_of(rb.pl, ob.J2a), nr = A.njt_of(rb.pr, jar);
+          int sl = get_slab(bl, rb.pl);
+          PendingOp op{sl, slabK[sl], (int)ai};
+          slabK[sl] += nr;
+          slab_blocks[sl].push_back({nr, rb.voff});
+          by_pr[rb.pr].push_back(op);
+          h->flops_a += 2.0 * nl * nr * ob.db;
+          h->flops_mix += 2.0 * nr * ob.db * G.ns;
+        }
+      }
+      for (auto &pp : by_pr)
+        for (size_t o0 = 0; o0 < pp.second.size(); o0 += ZMAXA) {
+          std::vector<PendingOp> part(pp.second.begin() + o0,
+                                      pp.second.begin() + std::min(pp.second.size(), o0 + (size_t)ZMAXA));
+          pending.push_back({gid, A.poff[A.jidx(jar)][pp.first], A.njt_of(pp.first, jar), part});
+        }
     }
-    for (auto &pp : by_pr) pending.push_back({gid, A.poff[A.jidx(jar)][pp.first], A.njt_of(pp.first, jar), pp.second});
   }
   // Zbar slabs and Abar
   std::vector<int64_t> zoff(slabs.size());
@@ -381,7 +397,6 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   for (auto &pd : pending) {
     const int bl = slabs[pd.ops[0].slab].first;
     const Block &ob = h->blocks[bl];
-    if (pd.ops.size() > (size_t)ZMAXA) fail(NSX_E_ARG, "too many proton operators on one partition");
     int op0 = (int)h->zops.size();
     for (const PendingOp &o : pd.ops) h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ob.db, o.wrow, 0});
     int op1 = (int)h->zops.size();
