@@ -55,6 +55,7 @@ struct Block {
 
 // ---- task lists of the H.v kernels -------------------------------------------
 // Y stage: Y_(h,b) = C_h * rho_b^T (row-major d_ar x d_bl), one group per (Y matrix, row tile).
+constexpr int KY_TILE_ROWS = 32;
 struct YGroup {
   int64_t c_base;   // element offset of input block h
   int64_t y_base;   // element offset of the Y matrix
@@ -158,7 +159,7 @@ struct nsx_handle {
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
   int64_t y_elems = 0, z_elems = 0;
-  int max_ynl = 0, max_ynr = 0, max_anl = 0;
+  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_ldy = 0;
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

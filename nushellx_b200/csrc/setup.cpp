@@ -291,7 +291,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     }
     int b1 = (int)h->yblks.size();
     h->flops_y += 2.0 * ib.da * nnz;
-    for (int r0 = 0; r0 < ib.da; r0 += 128)
+    for (int r0 = 0; r0 < ib.da; r0 += KY_TILE_ROWS)
       h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), 0});
   }
   // ---- stacked proton side: per output (block, P_l) the contributions (a, P_r) in a fixed
@@ -439,7 +439,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   }
   h->z_elems = ztot;
   h->y_elems = ytot;
-  h->max_ynl = h->max_ynr = h->max_anl = 0;
+  h->max_ynl = h->max_ynr = h->max_anl = h->max_ldy = 0;
+  for (auto &g : h->ygroups) h->max_ldy = std::max(h->max_ldy, g.ldy);
   for (auto &y : h->yblks) {
     h->max_ynl = std::max(h->max_ynl, y.nl);
     h->max_ynr = std::max(h->max_ynr, y.nr);
