@@ -86,49 +86,37 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 32-row tile); the tile (32 rows x d_bl columns,
-// row-major) is built in shared memory -- zero where no density block reaches --
-// and written out with coalesced row stores.  Thread t computes row t % 32 of
-// the density blocks t / 32, t / 32 + 8, ...
-constexpr int KY_ROWS = 32;
+// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
+// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T, the
+// density block and the C columns staged in shared memory; Y is row-major.
 template <typename T>
-__global__ void __launch_bounds__(256) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
-                                           const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
+__global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
+                                           const T *__restrict__ x, const T *__restrict__ rho,
+                                           T *__restrict__ Y, int max_nr, int max_nl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
+  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
   const YGroup g = groups[blockIdx.x];
-  const int ldt = g.ldy | 1;                       // odd stride: conflict-free column writes
-  T *tile = reinterpret_cast<T *>(smem_raw);      // [KY_ROWS][ldt]
-  const int nrow = min(KY_ROWS, g.m - g.row0);
-  for (int e = threadIdx.x; e < KY_ROWS * ldt; e += blockDim.x) tile[e] = T(0);
-  __syncthreads();
-  const int r = threadIdx.x % KY_ROWS, bsub = threadIdx.x / KY_ROWS;
-  const T *C = x + g.c_base + g.row0 + r;
-  if (r < nrow) {
-    for (int bi = g.b_begin + bsub; bi < g.b_end; bi += 256 / KY_ROWS) {
-      const YBlk b = blks[bi];
-      const T *Cb = C + (int64_t)g.m * b.ccol;
-      const T *R = rho + b.rho;
-      for (int l0 = 0; l0 < b.nl; l0 += 8) {
-        T acc[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = T(0);
-        for (int k = 0; k < b.nr; ++k) {
-          const T ck = Cb[(int64_t)g.m * k];
-          const T *Rk = R + (int64_t)b.nl * k + l0;
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (l0 + q < b.nl) acc[q] = fma(ck, __ldg(Rk + q), acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          if (l0 + q < b.nl) tile[r * ldt + b.ycol + l0 + q] = acc[q];
+  const int row = g.row0 + threadIdx.x;
+  const bool active = row < g.m;
+  const T *C = x + g.c_base;
+  T *Yr = Y + g.y_base + (int64_t)row * g.ldy;
+  for (int bi = g.b_begin; bi < g.b_end; ++bi) {
+    const YBlk b = blks[bi];
+    const int n = b.nl * b.nr;
+    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
+    if (active)
+      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
+    __syncthreads();
+    if (active) {
+      for (int l = 0; l < b.nl; ++l) {
+        T acc = T(0);
+        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
+        Yr[b.ycol + l] = acc;
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
-  T *Yg = Y + g.y_base + (int64_t)g.row0 * g.ldy;
-  for (int rr = 0; rr < nrow; ++rr)
-    for (int c = threadIdx.x; c < g.ldy; c += blockDim.x) Yg[(int64_t)rr * g.ldy + c] = tile[rr * ldt + c];
 }
 
 // ---------------------------------------------------------------------------
@@ -179,10 +167,12 @@ __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, cons
 }
 
 // ---------------------------------------------------------------------------
-// k_a: one CTA per (output slab P_l, 128-column tile); 256 threads = 4 row
-// slots x 64 column pairs; slot s owns rows [s*RPT, s*RPT + RPT) with RPT the
-// smallest of 1, 2, 4, 8, 16 that covers nl.  Abar is staged in shared memory
-// in chunks of KC stacked rows; each thread streams its two Zbar columns.
+// k_a: one CTA per (output slab P_l, 128-column tile, K range); 256 threads =
+// 4 row slots x 64 column pairs; slot s owns rows [s*RPT, s*RPT + RPT) with RPT
+// the smallest of 1, 2, 4, 8, 16 that covers nl.  Abar is staged in shared
+// memory in chunks of KC stacked rows; each thread streams its two Zbar
+// columns four rows at a time.  The K ranges of one tile add their partial
+// sums to the output with atomic adds (the like-particle stage wrote it first).
 constexpr int KA_KC = 128;
 template <typename T, int RPT>
 __device__ __forceinline__ void ka_body(const ATile &t, const T *__restrict__ Abar, const T *__restrict__ Zb,
@@ -190,21 +180,42 @@ __device__ __forceinline__ void ka_body(const ATile &t, const T *__restrict__ Ab
   const int nl = t.nl;
   const int rs = threadIdx.x / 64, cp = threadIdx.x % 64;
   const int c0 = 2 * cp, c1 = 2 * cp + 1;
+  const bool v0 = c0 < t.ncols, v1 = c1 < t.ncols;
   const int lb = rs * RPT;
   T acc0[RPT], acc1[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc0[j] = acc1[j] = T(0);
   const T *Z = Zb + t.zbar;
-  for (int k0 = 0; k0 < t.K; k0 += KA_KC) {
-    const int kc = min(KA_KC, t.K - k0);
+  for (int k0 = t.k_begin; k0 < t.k_end; k0 += KA_KC) {
+    const int kc = min(KA_KC, t.k_end - k0);
     const T *Ak = Abar + t.abar + (int64_t)k0 * nl;
     for (int e = threadIdx.x; e < kc * nl; e += blockDim.x) as[e] = Ak[e];
     __syncthreads();
     if (lb < nl) {
-      for (int k = 0; k < kc; ++k) {
+      int k = 0;
+      for (; k + 4 <= kc; k += 4) {
+        T z0[4], z1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const T *Zr = Z + (int64_t)(k0 + k + u) * t.ldz;
+          z0[u] = v0 ? Zr[c0] : T(0);
+          z1[u] = v1 ? Zr[c1] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const T *ak = as + (k + u) * nl + lb;
+#pragma unroll
+          for (int j = 0; j < RPT; ++j) {
+            const T a = (lb + j < nl) ? ak[j] : T(0);
+            acc0[j] = fma(a, z0[u], acc0[j]);
+            acc1[j] = fma(a, z1[u], acc1[j]);
+          }
+        }
+      }
+      for (; k < kc; ++k) {
         const T *Zr = Z + (int64_t)(k0 + k) * t.ldz;
-        const T z0 = c0 < t.ncols ? Zr[c0] : T(0);
-        const T z1 = c1 < t.ncols ? Zr[c1] : T(0);
+        const T z0 = v0 ? Zr[c0] : T(0);
+        const T z1 = v1 ? Zr[c1] : T(0);
         const T *ak = as + k * nl + lb;
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
@@ -220,8 +231,8 @@ __device__ __forceinline__ void ka_body(const ATile &t, const T *__restrict__ Ab
   for (int j = 0; j < RPT; ++j) {
     const int l = lb + j;
     if (l < nl) {
-      if (c0 < t.ncols) out[t.out + l + (int64_t)t.ld * c0] += acc0[j];
-      if (c1 < t.ncols) out[t.out + l + (int64_t)t.ld * c1] += acc1[j];
+      if (v0) atomicAdd(out + t.out + l + (int64_t)t.ld * c0, acc0[j]);
+      if (v1) atomicAdd(out + t.out + l + (int64_t)t.ld * c1, acc1[j]);
     }
   }
 }
@@ -274,7 +285,9 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ky_smem(const nsx_handle *h, size_t es) { return es * (size_t)KY_ROWS * (h->max_ldy | 1); }
+static size_t ky_smem(const nsx_handle *h, size_t es) {
+  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
+}
 static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 void upload(nsx_handle *h) {
@@ -315,11 +328,13 @@ void ensure_precision(nsx_handle *h, int precision) {
   if (precision == NSX_FP64) {
     if (!d.y64) {
       NSX_CUDA(cudaMalloc(&d.y64, ny * sizeof(double)));
+      NSX_CUDA(cudaMemset(d.y64, 0, ny * sizeof(double)));  // column slabs no density block reaches stay zero
       NSX_CUDA(cudaMalloc(&d.z64, nz * sizeof(double)));
     }
   } else if (precision == NSX_FP32) {
     if (!d.y32) {
       NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
+      NSX_CUDA(cudaMemset(d.y32, 0, ny * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.z32, nz * sizeof(float)));
       d.rhoA32 = dev_copy<float>(h->A.vals);
       d.rhoB32 = dev_copy<float>(h->B.vals);
@@ -401,7 +416,8 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->ygroups.empty()) {
     StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 256, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y);
+    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
+                                                                             h->max_ynr, h->max_ynl);
   }
   if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);

@@ -55,7 +55,8 @@ struct Block {
 
 // ---- task lists of the H.v kernels -------------------------------------------
 // Y stage: Y_(h,b) = C_h * rho_b^T (row-major d_ar x d_bl), one group per (Y matrix, row tile).
-constexpr int KY_TILE_ROWS = 32;
+constexpr int KY_TILE_ROWS = 128;
+constexpr int KA_K_SPLIT = 512;   // stacked rows per k_a tile (longer slabs are split, partial sums added atomically)
 struct YGroup {
   int64_t c_base;   // element offset of input block h
   int64_t y_base;   // element offset of the Y matrix
@@ -103,7 +104,7 @@ struct ATile {
   int32_t nl;       // rows = nJT(P_l, J_al)
   int32_t col0, ncols;
   int32_t ldz;      // d_bl
-  int32_t K;        // stacked contribution rows
+  int32_t k_begin, k_end;  // range of stacked contribution rows handled by this tile
   int64_t zbar;     // offset of Zbar[0, col0]
   int64_t abar;     // offset of Abar[0, 0]
 };

@@ -423,20 +423,26 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       int nl = A.njt_of(pl, ob.J2a);
       h->abar.insert(h->abar.end(), A.vals.begin() + bv.second, A.vals.begin() + bv.second + (int64_t)nl * bv.first);
     }
-    for (int c0 = 0; c0 < ob.db; c0 += TW) {
-      ATile t;
-      t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
-      t.ld = ob.da;
-      t.nl = A.njt_of(pl, ob.J2a);
-      t.col0 = c0;
-      t.ncols = std::min(TW, ob.db - c0);
-      t.ldz = ob.db;
-      t.zbar = zoff[sl] + c0;
-      t.abar = a0;
-      t.K = slabK[sl];
-      h->atiles.push_back(t);
-    }
+    for (int c0 = 0; c0 < ob.db; c0 += TW)
+      for (int kb = 0; kb < slabK[sl]; kb += KA_K_SPLIT) {
+        ATile t;
+        t.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)c0 * ob.da;
+        t.ld = ob.da;
+        t.nl = A.njt_of(pl, ob.J2a);
+        t.col0 = c0;
+        t.ncols = std::min(TW, ob.db - c0);
+        t.ldz = ob.db;
+        t.k_begin = kb;
+        t.k_end = std::min(slabK[sl], kb + KA_K_SPLIT);
+        t.zbar = zoff[sl] + c0;
+        t.abar = a0;
+        h->atiles.push_back(t);
+      }
   }
+  // longest tiles first
+  std::stable_sort(h->atiles.begin(), h->atiles.end(), [](const ATile &x, const ATile &y) {
+    return (int64_t)(x.k_end - x.k_begin) * x.nl > (int64_t)(y.k_end - y.k_begin) * y.nl;
+  });
   h->z_elems = ztot;
   h->y_elems = ytot;
   h->max_ynl = h->max_ynr = h->max_anl = h->max_ldy = 0;
