@@ -16,10 +16,10 @@
 //   that first call before any stream capture.  Every GPU that loads the
 //   library holds the array until the process exits.
 // * All calls share the one array and it keeps the last call's contents; the
-//   product writes every element it later reads (zero where no density block
-//   reaches), so nothing is cleared between calls.  Calls that overlap on the
-//   GPU (different streams, or different handles on the same device, without
-//   ordering) race on the array.
+//   part the product needs zeroed (the Y slabs no density block reaches) is
+//   cleared at the start of every call on the caller's stream.  Calls that
+//   overlap on the GPU (different streams, or different handles on the same
+//   device, without ordering) race on the array.
 #include <mutex>
 #include "nsx_internal.h"
 
@@ -60,7 +60,9 @@ int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream
   NSX_CUDA(cudaSetDevice(h->device));
   double *Y = noalloc_scratch(h->device);
   cudaStream_t s = (cudaStream_t)stream;
-  // the array holds Y then Zbar; every element of both is written by the product before it is read
+  // the array holds Y then Zbar; column slabs of Y that no density block reaches are read as
+  // zeros by the mixing stage and are never written, so the Y part is cleared on every call
+  if (h->y_elems > 0) NSX_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)h->y_elems, s));
   matvec_fp64_with_scratch(h, x, y, Y, s);
   return NSX_OK;
 }
