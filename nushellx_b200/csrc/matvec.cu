@@ -86,47 +86,36 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  The neutron density
-// key's values are staged in shared memory once; then, without further
-// barriers, each thread computes Y[row, Q_l cols] = C[row, Q_r cols] rho^T for
-// every sub-block (Q_l, Q_r), four outputs at a time with its C values held in
-// registers.  Y is row-major.
+// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
+// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T, the
+// density block and the C columns staged in shared memory; Y is row-major.
 template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
-                                           const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
+                                           const T *__restrict__ x, const T *__restrict__ rho,
+                                           T *__restrict__ Y, int max_nr, int max_nl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *rs = reinterpret_cast<T *>(smem_raw);  // the key's density values
+  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
+  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
   const YGroup g = groups[blockIdx.x];
-  for (int e = threadIdx.x; e < g.rho_n; e += blockDim.x) rs[e] = rho[g.rho_base + e];
-  __syncthreads();
   const int row = g.row0 + threadIdx.x;
-  if (row >= g.m) return;
-  const T *C = x + g.c_base + row;
+  const bool active = row < g.m;
+  const T *C = x + g.c_base;
   T *Yr = Y + g.y_base + (int64_t)row * g.ldy;
   for (int bi = g.b_begin; bi < g.b_end; ++bi) {
     const YBlk b = blks[bi];
-    const T *Cb = C + (int64_t)g.m * b.ccol;
-    const T *R = rs + b.rho;  // relative to the key's first value
-    for (int l0 = 0; l0 < b.nl; l0 += 4) {
-      T acc[4] = {T(0), T(0), T(0), T(0)};
-      for (int k0 = 0; k0 < b.nr; k0 += 8) {
-        T ck[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) ck[j] = (k0 + j < b.nr) ? Cb[(int64_t)g.m * (k0 + j)] : T(0);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (k0 + j < b.nr) {
-            const T *Rk = R + b.nl * (k0 + j) + l0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              if (l0 + q < b.nl) acc[q] = fma(ck[j], Rk[q], acc[q]);
-          }
-        }
+    const int n = b.nl * b.nr;
+    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
+    if (active)
+      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
+    __syncthreads();
+    if (active) {
+      for (int l = 0; l < b.nl; ++l) {
+        T acc = T(0);
+        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
+        Yr[b.ycol + l] = acc;
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (l0 + q < b.nl) Yr[b.ycol + l0 + q] = acc[q];
     }
+    __syncthreads();
   }
 }
 
@@ -296,7 +285,9 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ky_smem(const nsx_handle *h, size_t es) { return es * (size_t)std::max(h->max_key_vals, 1); }
+static size_t ky_smem(const nsx_handle *h, size_t es) {
+  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
+}
 static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 void upload(nsx_handle *h) {
@@ -425,7 +416,8 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->ygroups.empty()) {
     StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y);
+    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
+                                                                             h->max_ynr, h->max_ynl);
   }
   if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);

@@ -64,11 +64,10 @@ struct YGroup {
   int32_t row0;     // first row of the tile
   int32_t b_begin, b_end;  // range in yblks
   int32_t ldy;      // d_bl (row length of Y)
-  int32_t rho_n;    // number of values of the neutron density key (staged in shared memory)
-  int64_t rho_base; // offset of the key's first value
+  int32_t pad;
 };
 struct YBlk {
-  int64_t rho;      // offset of the nl x nr (column-major) density sub-block, relative to the key's first value
+  int64_t rho;      // offset of the nl x nr (column-major) density sub-block
   int32_t ccol;     // first column of C_h (right partition Q_r)
   int32_t ycol;     // first column of Y (left partition Q_l)
   int32_t nl, nr;
@@ -161,7 +160,7 @@ struct nsx_handle {
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
   int64_t y_elems = 0, z_elems = 0;
-  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_ldy = 0, max_key_vals = 0;
+  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_ldy = 0;
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -273,31 +273,26 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   h->ygroups.clear();
   h->yblks.clear();
   h->flops_y = 0;
-  h->max_key_vals = 0;
   for (size_t y = 0; y < ymats.size(); ++y) {
     int hb = ymats[y].first, bk = ymats[y].second;
     const Block &ib = h->blocks[hb];
     int J2bl = (int)(B.keys[bk] & 255), J2br = (int)((B.keys[bk] >> 8) & 255);
     int b0 = (int)h->yblks.size();
     double nnz = 0;
-    int64_t kbase = B.kblocks[bk].front().voff, kend = kbase;
     for (const RhoBlk &rb : B.kblocks[bk]) {
       YBlk yb;
-      yb.rho = rb.voff - kbase;
+      yb.rho = rb.voff;
       yb.ccol = B.poff[B.jidx(J2br)][rb.pr];
       yb.ycol = B.poff[B.jidx(J2bl)][rb.pl];
       yb.nl = B.njt_of(rb.pl, J2bl);
       yb.nr = B.njt_of(rb.pr, J2br);
       nnz += (double)yb.nl * yb.nr;
-      kend = std::max(kend, rb.voff + (int64_t)yb.nl * yb.nr);
       h->yblks.push_back(yb);
     }
     int b1 = (int)h->yblks.size();
-    const int nvals = (int)(kend - kbase);
-    h->max_key_vals = std::max(h->max_key_vals, nvals);
     h->flops_y += 2.0 * ib.da * nnz;
     for (int r0 = 0; r0 < ib.da; r0 += KY_TILE_ROWS)
-      h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), nvals, kbase});
+      h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), 0});
   }
   // ---- stacked proton side: per output (block, P_l) the contributions (a, P_r) in a fixed
   // order; Abar = their density blocks side by side (nl x K column-major), Zbar = K x d_bl
