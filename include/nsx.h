@@ -144,8 +144,8 @@ int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, voi
 /* y = H x in FP64 without allocating device memory (no counterpart in the
  * reference).  For callers that cannot have device memory allocated during
  * the call: cudaMalloc synchronises the whole device, and some hosts give all
- * device memory to their own pool.  The Y intermediates go to a fixed
- * file-scope device array of 8 Mi FP64 elements (64 MiB, held by every GPU
+ * device memory to their own pool.  The intermediates (Y and the stacked
+ * Zbar) go to a fixed file-scope device array of 8 Mi FP64 elements (64 MiB, held by every GPU
  * that loads the library until exit); larger problems are rejected with
  * NSX_E_ARG.  The first call on a device looks up the array's address: make it
  * before any stream capture.  All calls share the array; calls that overlap on

@@ -1,0 +1,153 @@
+! nsx_iface.f90 -- Fortran 2003 iso_c_binding interface to libnsx (include/nsx.h).
+!
+! For NuShellX's Fortran host code (NuLnz / NuTRL): the module gives the
+! bind(C) types and interfaces of every entry point, so that Lnz_TRD's set-up
+! (src/NuLnz/NuCoreX.f90:807-1367), the multiplyx/multiplya/multiplyb product
+! (NuCoreX.f90:76-226) and Lnz_OP (NuCoreX.f90:240-751) can be replaced by calls
+! into the B200 library.  Column-major Fortran arrays of real(8) map directly to
+! the library's vector layout (blocks (2Ja,2Jb) in ascending order, each a
+! d_a x d_b column-major matrix).  Compile with any Fortran 2003 compiler and
+! link against nushellx_b200/libnsx.so.  (This machine has no Fortran compiler,
+! so the module is not compiled here; the C header is the authoritative ABI.)
+module nsx_iface
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: NSX_OK = 0, NSX_E_ARG = -1, NSX_E_IO = -2, NSX_E_CUDA = -3, &
+                               NSX_E_NOMEM = -4, NSX_E_NUMERIC = -5, NSX_E_NOCONV = -6
+  integer(c_int), parameter :: NSX_FP64 = 0, NSX_FP32 = 1
+  integer(c_int), parameter :: NSX_STAGES = 5
+
+  type, bind(C) :: nsx_species
+     integer(c_int32_t) :: nspart, minJ2, maxJ2
+     type(c_ptr)        :: njt, parity
+     integer(c_int32_t) :: shell_first, nshell
+     integer(c_int32_t) :: nkeys
+     type(c_ptr)        :: keys, val_off, vals
+     integer(c_int32_t) :: words
+     type(c_ptr)        :: masks
+     integer(c_int32_t) :: nseg
+     type(c_ptr)        :: seg_J2, seg_np, seg_npr, seg_off, seg_vals
+  end type nsx_species
+
+  type, bind(C) :: nsx_problem
+     integer(c_int32_t) :: J2, parity
+     type(nsx_species)  :: a, b
+     integer(c_int32_t) :: nop
+     type(c_ptr)        :: op_keys, op_vals
+     real(c_double)     :: renorm
+  end type nsx_problem
+
+  type, bind(C) :: nsx_files
+     type(c_ptr)        :: a, b, inter, like_a, like_b   ! NUL-terminated base names
+     integer(c_int32_t) :: T2_a, nmp_a, T2_b, nmp_b
+     character(kind=c_char) :: xtra
+     integer(c_int32_t) :: J2, parity, nshells, nshells_p
+     type(c_ptr)        :: shell_parity
+  end type nsx_files
+
+  type, bind(C) :: nsx_params
+     integer(c_int32_t) :: nev, max_iter, window, keep
+     real(c_double)     :: tol
+     integer(c_int32_t) :: precision, pre_iter
+     integer(c_int64_t) :: seed
+     type(c_ptr)        :: start
+     integer(c_int32_t) :: refine
+  end type nsx_params
+
+  type, bind(C) :: nsx_report
+     integer(c_int32_t) :: iterations, matvecs, restarts, converged
+     real(c_double)     :: seconds, matvec_seconds
+     real(c_double)     :: residual(64)
+  end type nsx_report
+
+  type, bind(C) :: nsx_stats
+     integer(c_int64_t) :: launches, matvecs
+     integer(c_int64_t) :: stage_launches(NSX_STAGES)
+     real(c_double)     :: stage_ms(NSX_STAGES), stage_bytes(NSX_STAGES), stage_flops(NSX_STAGES)
+  end type nsx_stats
+
+  interface
+     integer(c_int) function nsx_create(prob, device, out) bind(C, name="nsx_create")
+       import :: c_int, c_ptr, nsx_problem
+       type(nsx_problem), intent(in) :: prob
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_load_files(files, device, out) bind(C, name="nsx_load_files")
+       import :: c_int, c_ptr, nsx_files
+       type(nsx_files), intent(in) :: files
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_file_code(i, j, k, code) bind(C, name="nsx_file_code")
+       import :: c_int, c_int32_t, c_char
+       integer(c_int32_t), value :: i, j, k
+       character(kind=c_char), intent(out) :: code(4)
+     end function
+     integer(c_int64_t) function nsx_dim(h) bind(C, name="nsx_dim")
+       import :: c_int64_t, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int32_t) function nsx_nblocks(h) bind(C, name="nsx_nblocks")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function nsx_blocks(h, blocks4, offsets) bind(C, name="nsx_blocks")
+       import :: c_int, c_int32_t, c_int64_t, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int32_t), intent(out) :: blocks4(*)
+       integer(c_int64_t), intent(out) :: offsets(*)
+     end function
+     integer(c_int) function nsx_lcoef(h, mask) bind(C, name="nsx_lcoef")
+       import :: c_int, c_int8_t, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int8_t), intent(out) :: mask(*)
+     end function
+     real(c_double) function nsx_matvec_flops(h) bind(C, name="nsx_matvec_flops")
+       import :: c_double, c_ptr
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function nsx_matvec(h, x, y, precision, stream) bind(C, name="nsx_matvec")
+       import :: c_int, c_int32_t, c_ptr
+       type(c_ptr), value :: h, x, y, stream           ! x, y: device pointers
+       integer(c_int32_t), value :: precision
+     end function
+     integer(c_int) function nsx_matvec_noalloc(h, x, y, stream) bind(C, name="nsx_matvec_noalloc")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, x, y, stream           ! x, y: device pointers, FP64
+     end function
+     integer(c_int) function nsx_matvec_host(h, x, y, precision) bind(C, name="nsx_matvec_host")
+       import :: c_int, c_int32_t, c_double, c_ptr
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: x(*)              ! the reference's coefR
+       real(c_double), intent(out) :: y(*)             ! the reference's coefL
+       integer(c_int32_t), value :: precision
+     end function
+     integer(c_int) function nsx_solve(h, params, evals, evecs, report) bind(C, name="nsx_solve")
+       import :: c_int, c_double, c_ptr, nsx_params, nsx_report
+       type(c_ptr), value :: h
+       type(nsx_params), intent(in) :: params
+       real(c_double), intent(out) :: evals(*)
+       type(c_ptr), value :: evecs                     ! c_loc(vectors(1,1)) or c_null_ptr
+       type(nsx_report), intent(out) :: report
+     end function
+     integer(c_int) function nsx_stats_reset(h, timing) bind(C, name="nsx_stats_reset")
+       import :: c_int, c_int32_t, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int32_t), value :: timing
+     end function
+     integer(c_int) function nsx_get_stats(h, stats) bind(C, name="nsx_get_stats")
+       import :: c_int, c_ptr, nsx_stats
+       type(c_ptr), value :: h
+       type(nsx_stats), intent(out) :: stats
+     end function
+     subroutine nsx_destroy(h) bind(C, name="nsx_destroy")
+       import :: c_ptr
+       type(c_ptr), value :: h
+     end subroutine
+     type(c_ptr) function nsx_last_error() bind(C, name="nsx_last_error")
+       import :: c_ptr
+     end function
+  end interface
+end module nsx_iface

@@ -73,3 +73,33 @@ def test_missing_files_report_io_error(lib, tmp_path):
     rc = lib.nsx_load_files(ctypes.byref(f), 0, ctypes.byref(h))
     assert rc == -2
     assert b"cannot open" in lib.nsx_last_error()
+
+
+def test_fortran_interface_binds_every_entry_point():
+    text = open(os.path.join(ROOT, "include", "nsx_iface.f90")).read()
+    bound = set(re.findall(r'bind\(C, name="(nsx_[a-z0-9_]+)"\)', text))
+    assert bound == set(declared_functions())
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """sizeof/offsetof of every ABI struct from the C compiler equals the Python binding's."""
+    import ctypes
+    from nushellx_b200 import nsx
+    structs = {"nsx_species": nsx.Species, "nsx_problem": nsx.Problem, "nsx_params": nsx.Params,
+               "nsx_report": nsx.Report, "nsx_files": nsx.Files, "nsx_stats": nsx.Stats}
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "nsx.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            src.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    src.append("return 0; }")
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(out[f"{cname}.{fname}"]) == getattr(py, fname).offset, (cname, fname)
