@@ -87,42 +87,35 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 
 // ---------------------------------------------------------------------------
 // k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
-// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T, four
-// outputs at a time, the row's C values in registers (8 per chunk, coalesced
-// across the warp) and the density values read as warp-uniform loads (L1
-// broadcasts).  No shared memory, no barriers.  Y is row-major.
+// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T, the
+// density block and the C columns staged in shared memory; Y is row-major.
 template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
-                                           const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
+                                           const T *__restrict__ x, const T *__restrict__ rho,
+                                           T *__restrict__ Y, int max_nr, int max_nl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
+  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
   const YGroup g = groups[blockIdx.x];
   const int row = g.row0 + threadIdx.x;
-  if (row >= g.m) return;
-  const T *C = x + g.c_base + row;
+  const bool active = row < g.m;
+  const T *C = x + g.c_base;
   T *Yr = Y + g.y_base + (int64_t)row * g.ldy;
   for (int bi = g.b_begin; bi < g.b_end; ++bi) {
     const YBlk b = blks[bi];
-    const T *Cb = C + (int64_t)g.m * b.ccol;
-    const T *R = rho + b.rho;
-    for (int l0 = 0; l0 < b.nl; l0 += 4) {
-      T acc[4] = {T(0), T(0), T(0), T(0)};
-      for (int k0 = 0; k0 < b.nr; k0 += 8) {
-        T ck[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) ck[j] = (k0 + j < b.nr) ? Cb[(int64_t)g.m * (k0 + j)] : T(0);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (k0 + j < b.nr) {
-            const T *Rk = R + (int64_t)b.nl * (k0 + j) + l0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              if (l0 + q < b.nl) acc[q] = fma(ck[j], __ldg(Rk + q), acc[q]);
-          }
-        }
+    const int n = b.nl * b.nr;
+    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
+    if (active)
+      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
+    __syncthreads();
+    if (active) {
+      for (int l = 0; l < b.nl; ++l) {
+        T acc = T(0);
+        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
+        Yr[b.ycol + l] = acc;
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (l0 + q < b.nl) Yr[b.ycol + l0 + q] = acc[q];
     }
+    __syncthreads();
   }
 }
 
@@ -292,7 +285,9 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ky_smem(const nsx_handle *, size_t) { return 0; }
+static size_t ky_smem(const nsx_handle *h, size_t es) {
+  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
+}
 static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 void upload(nsx_handle *h) {
@@ -321,7 +316,9 @@ void upload(nsx_handle *h) {
     if (ky_smem(h, es) > 227 * 1024 || ka_smem(h, es) > 227 * 1024)
       fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_y / k_a");
   }
+  NSX_CUDA(cudaFuncSetAttribute(k_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 8)));
   NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 8)));
+  NSX_CUDA(cudaFuncSetAttribute(k_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 4)));
   NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 4)));
 }
 
@@ -419,7 +416,8 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->ygroups.empty()) {
     StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 128, 0, s>>>(d.ygroups, d.yblks, x, rhoB, Y);
+    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
+                                                                             h->max_ynr, h->max_ynl);
   }
   if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);
