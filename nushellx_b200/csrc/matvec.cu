@@ -86,34 +86,116 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 128-row tile); thread = row.  For each neutron
-// density sub-block (Q_l, Q_r): Y[row, Q_l cols] = C[row, Q_r cols] rho^T, the
-// density block and the C columns staged in shared memory; Y is row-major.
+// k_y: one CTA per (Y matrix, 256-row tile); thread = two rows (t, t + 128).
+// The tile's part of Y (256 consecutive rows of a row-major matrix) is produced
+// in column windows of 128 bytes (32 FP32 / 16 FP64 columns): every neutron
+// density sub-block (Q_l, Q_r) overlapping the window adds
+//   Y[row, Q_l cols] = C[row, Q_r cols] rho^T
+// into a padded shared-memory tile, the row's C values held in registers (up to 8
+// per chunk, coalesced loads) and the density values read as warp-uniform 16-byte
+// loads (4 outputs x 2 rows = 8 FMAs per coefficient).  The window is then written
+// out with coalesced row segments and cleared in the same pass.  Every element of
+// Y is written, so Y needs no clearing between products.
+template <typename T> struct KyWin;
+template <> struct KyWin<float> { static constexpr int W = 32; };
+template <> struct KyWin<double> { static constexpr int W = 16; };
+
+__device__ __forceinline__ void ky_load4(const float *p, float v[4]) {
+  const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ky_load4(const double *p, double v[4]) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// Adds the contribution of density columns [k0, k0 + KC) of one sub-block to the
+// tile columns of outputs l in [lo, hi) (relative to the sub-block), for both rows.
+template <typename T, int KC>
+__device__ __forceinline__ void ky_chunk(const T *__restrict__ c0p, const T *__restrict__ c1p, bool ok0, bool ok1,
+                                         int64_t m, const T *__restrict__ R, int ldr, int lo, int hi, T *t0, T *t1) {
+  T c0[KC], c1[KC];
+#pragma unroll
+  for (int j = 0; j < KC; ++j) {
+    c0[j] = ok0 ? c0p[m * j] : T(0);
+    c1[j] = ok1 ? c1p[m * j] : T(0);
+  }
+  for (int g = lo & ~3; g < hi; g += 4) {
+    T a0[4] = {T(0), T(0), T(0), T(0)}, a1[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      T v[4];
+      ky_load4(R + (int64_t)ldr * j + g, v);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a0[q] = fma(c0[j], v[q], a0[q]);
+        a1[q] = fma(c1[j], v[q], a1[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int l = g + q;
+      if (l >= lo && l < hi) {
+        t0[l] += a0[q];
+        t1[l] += a1[q];
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
-                                           const T *__restrict__ x, const T *__restrict__ rho,
-                                           T *__restrict__ Y, int max_nr, int max_nl) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *rs = reinterpret_cast<T *>(smem_raw);          // [max_nl*max_nr]
-  T *cs = rs + (size_t)max_nl * max_nr;             // [max_nr][128]
+                                           const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
+  constexpr int W = KyWin<T>::W;
+  constexpr int LD = W + 1;
+  __shared__ T tile[KY_TILE_ROWS * LD];
   const YGroup g = groups[blockIdx.x];
-  const int row = g.row0 + threadIdx.x;
-  const bool active = row < g.m;
+  const int tid = threadIdx.x;
+  const int r0 = g.row0 + tid, r1 = r0 + 128;
+  const bool ok0 = r0 < g.m, ok1 = r1 < g.m;
+  const int64_t m = g.m;
   const T *C = x + g.c_base;
-  T *Yr = Y + g.y_base + (int64_t)row * g.ldy;
-  for (int bi = g.b_begin; bi < g.b_end; ++bi) {
-    const YBlk b = blks[bi];
-    const int n = b.nl * b.nr;
-    for (int e = threadIdx.x; e < n; e += 128) rs[e] = rho[b.rho + e];
-    if (active)
-      for (int k = 0; k < b.nr; ++k) cs[k * 128 + threadIdx.x] = C[row + (int64_t)g.m * (b.ccol + k)];
-    __syncthreads();
-    if (active) {
-      for (int l = 0; l < b.nl; ++l) {
-        T acc = T(0);
-        for (int k = 0; k < b.nr; ++k) acc = fma(cs[k * 128 + threadIdx.x], rs[l + b.nl * k], acc);
-        Yr[b.ycol + l] = acc;
+  for (int e = tid; e < KY_TILE_ROWS * LD; e += 128) tile[e] = T(0);
+  __syncthreads();
+  const int rows = min(KY_TILE_ROWS, g.m - g.row0);
+  T *Yt = Y + g.y_base + (int64_t)g.row0 * g.ldy;
+  int bi = g.b_begin;
+  for (int w0 = 0; w0 < g.ldy; w0 += W) {
+    const int w1 = min(w0 + W, g.ldy);
+    while (bi < g.b_end && blks[bi].ycol + blks[bi].nl <= w0) ++bi;
+    for (int bj = bi; bj < g.b_end; ++bj) {
+      const YBlk b = blks[bj];
+      if (b.ycol >= w1) break;
+      const int lo = max(0, w0 - b.ycol), hi = min(b.nl, w1 - b.ycol);
+      // tile column of output l is b.ycol + l - w0
+      T *t0 = tile + tid * LD + (b.ycol - w0);
+      T *t1 = tile + (tid + 128) * LD + (b.ycol - w0);
+      const T *cb0 = C + r0 + m * b.ccol, *cb1 = C + r1 + m * b.ccol;
+      const T *R = rho + b.rho;
+      for (int k0 = 0; k0 < b.nr; k0 += 8) {
+        const int kc = min(8, b.nr - k0);
+        const T *c0p = cb0 + m * k0, *c1p = cb1 + m * k0;
+        const T *Rk = R + (int64_t)b.ldr * k0;
+        switch (kc) {
+          case 1: ky_chunk<T, 1>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 2: ky_chunk<T, 2>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 3: ky_chunk<T, 3>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 4: ky_chunk<T, 4>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 5: ky_chunk<T, 5>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 6: ky_chunk<T, 6>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          case 7: ky_chunk<T, 7>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+          default: ky_chunk<T, 8>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
+        }
       }
+    }
+    __syncthreads();
+    const int wn = w1 - w0;
+    for (int e = tid; e < rows * W; e += 128) {
+      const int r = e / W, c = e - r * W;
+      T *tp = tile + r * LD + c;
+      if (c < wn) Yt[(int64_t)r * g.ldy + w0 + c] = *tp;
+      *tp = T(0);
     }
     __syncthreads();
   }
@@ -285,9 +367,6 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ky_smem(const nsx_handle *h, size_t es) {
-  return es * ((size_t)h->max_ynl * h->max_ynr + (size_t)h->max_ynr * 128);
-}
 static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 void upload(nsx_handle *h) {
@@ -295,7 +374,7 @@ void upload(nsx_handle *h) {
   if (h->max_anl > 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
   d.rhoA = dev_copy<double>(h->A.vals);
-  d.rhoB = dev_copy<double>(h->B.vals);
+  d.rhoB = dev_copy<double>(h->yrho);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
   d.w = dev_copy<double>(h->weights);
@@ -313,12 +392,9 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
   for (size_t es : {sizeof(double), sizeof(float)}) {
-    if (ky_smem(h, es) > 227 * 1024 || ka_smem(h, es) > 227 * 1024)
-      fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_y / k_a");
+    if (ka_smem(h, es) > 227 * 1024) fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_a");
   }
-  NSX_CUDA(cudaFuncSetAttribute(k_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 8)));
   NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 8)));
-  NSX_CUDA(cudaFuncSetAttribute(k_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ky_smem(h, 4)));
   NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 4)));
 }
 
@@ -328,16 +404,14 @@ void ensure_precision(nsx_handle *h, int precision) {
   if (precision == NSX_FP64) {
     if (!d.y64) {
       NSX_CUDA(cudaMalloc(&d.y64, ny * sizeof(double)));
-      NSX_CUDA(cudaMemset(d.y64, 0, ny * sizeof(double)));  // column slabs no density block reaches stay zero
       NSX_CUDA(cudaMalloc(&d.z64, nz * sizeof(double)));
     }
   } else if (precision == NSX_FP32) {
     if (!d.y32) {
       NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
-      NSX_CUDA(cudaMemset(d.y32, 0, ny * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.z32, nz * sizeof(float)));
       d.rhoA32 = dev_copy<float>(h->A.vals);
-      d.rhoB32 = dev_copy<float>(h->B.vals);
+      d.rhoB32 = dev_copy<float>(h->yrho);
       d.hA32 = dev_copy<float>(h->A.hdense);
       d.hB32 = dev_copy<float>(h->B.hdense);
       d.w32 = dev_copy<float>(h->weights);
@@ -416,8 +490,7 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->ygroups.empty()) {
     StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 128, ky_smem(h, sizeof(T)), s>>>(d.ygroups, d.yblks, x, rhoB, Y,
-                                                                             h->max_ynr, h->max_ynl);
+    k_y<T><<<(unsigned)h->ygroups.size(), 128, 0, s>>>(d.ygroups, d.yblks, x, rhoB, Y);
   }
   if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);

@@ -60,9 +60,8 @@ int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream
   NSX_CUDA(cudaSetDevice(h->device));
   double *Y = noalloc_scratch(h->device);
   cudaStream_t s = (cudaStream_t)stream;
-  // the array holds Y then Zbar; column slabs of Y that no density block reaches are read as
-  // zeros by the mixing stage and are never written, so the Y part is cleared on every call
-  if (h->y_elems > 0) NSX_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)h->y_elems, s));
+  // the array holds Y then Zbar; the Y stage writes every element of Y (zeros where no density
+  // block reaches) and the mixing stage every element of Zbar, so nothing is cleared beforehand
   matvec_fp64_with_scratch(h, x, y, Y, s);
   return NSX_OK;
 }

@@ -55,7 +55,11 @@ struct Block {
 
 // ---- task lists of the H.v kernels -------------------------------------------
 // Y stage: Y_(h,b) = C_h * rho_b^T (row-major d_ar x d_bl), one group per (Y matrix, row tile).
-constexpr int KY_TILE_ROWS = 128;
+// The densities are re-laid out for it: every sub-block starts at a multiple of 4 elements and
+// has its leading dimension rounded up to a multiple of 4 (zero padding), so that groups of 4
+// outputs load their coefficients with 16-byte vector loads in FP32 and FP64.
+constexpr int KY_TILE_ROWS = 256;  // 128 threads x 2 rows
+constexpr int KY_PAD = 4;
 constexpr int KA_K_SPLIT = 512;   // stacked rows per k_a tile (longer slabs are split, partial sums added atomically)
 struct YGroup {
   int64_t c_base;   // element offset of input block h
@@ -67,10 +71,12 @@ struct YGroup {
   int32_t pad;
 };
 struct YBlk {
-  int64_t rho;      // offset of the nl x nr (column-major) density sub-block
+  int64_t rho;      // offset of the nl x nr (column-major, leading dimension ldr) padded density sub-block
   int32_t ccol;     // first column of C_h (right partition Q_r)
-  int32_t ycol;     // first column of Y (left partition Q_l)
+  int32_t ycol;     // first column of Y (left partition Q_l); blocks of one Y matrix ascend in ycol
   int32_t nl, nr;
+  int32_t ldr;      // nl rounded up to KY_PAD
+  int32_t pad;
 };
 // Mixing stage k_z: Z_a[P_r rows] = sum_s w_(a,s) Y_s[P_r rows] for the proton operators a of a
 // group (output block, J_ar, lam) acting on P_r; written into the stacked operand Zbar.
@@ -157,6 +163,7 @@ struct nsx_handle {
   std::vector<nsx::ZOp> zops;
   std::vector<nsx::ATile> atiles;
   std::vector<double> abar;
+  std::vector<double> yrho;        // padded neutron densities read by the Y stage
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
   int64_t y_elems = 0, z_elems = 0;

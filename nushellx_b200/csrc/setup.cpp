@@ -272,7 +272,9 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     for (const Entry &e : r.e) get_ymat(e.hb, e.bk);
   h->ygroups.clear();
   h->yblks.clear();
+  h->yrho.clear();
   h->flops_y = 0;
+  std::unordered_map<int64_t, int64_t> yrho_at;  // .trd value offset -> padded offset
   for (size_t y = 0; y < ymats.size(); ++y) {
     int hb = ymats[y].first, bk = ymats[y].second;
     const Block &ib = h->blocks[hb];
@@ -281,15 +283,29 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     double nnz = 0;
     for (const RhoBlk &rb : B.kblocks[bk]) {
       YBlk yb;
-      yb.rho = rb.voff;
       yb.ccol = B.poff[B.jidx(J2br)][rb.pr];
       yb.ycol = B.poff[B.jidx(J2bl)][rb.pl];
       yb.nl = B.njt_of(rb.pl, J2bl);
       yb.nr = B.njt_of(rb.pr, J2br);
+      yb.ldr = (yb.nl + KY_PAD - 1) / KY_PAD * KY_PAD;
+      yb.pad = 0;
+      auto it = yrho_at.find(rb.voff);
+      if (it == yrho_at.end()) {
+        int64_t at = (int64_t)h->yrho.size();
+        h->yrho.resize(at + (size_t)yb.ldr * yb.nr, 0.0);
+        for (int k = 0; k < yb.nr; ++k)
+          for (int l = 0; l < yb.nl; ++l) h->yrho[at + (size_t)yb.ldr * k + l] = B.vals[rb.voff + (size_t)yb.nl * k + l];
+        it = yrho_at.emplace(rb.voff, at).first;
+      }
+      yb.rho = it->second;
       nnz += (double)yb.nl * yb.nr;
       h->yblks.push_back(yb);
     }
     int b1 = (int)h->yblks.size();
+    std::sort(h->yblks.begin() + b0, h->yblks.end(), [](const YBlk &u, const YBlk &v) { return u.ycol < v.ycol; });
+    for (int i = b0 + 1; i < b1; ++i)
+      if (h->yblks[i].ycol < h->yblks[i - 1].ycol + h->yblks[i - 1].nl)
+        fail(NSX_E_ARG, "neutron density sub-blocks of one operator overlap in their left partition");
     h->flops_y += 2.0 * ib.da * nnz;
     for (int r0 = 0; r0 < ib.da; r0 += KY_TILE_ROWS)
       h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), 0});
