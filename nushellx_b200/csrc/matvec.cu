@@ -86,61 +86,74 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 256-row tile); thread = two rows (t, t + 128).
+// k_y: one CTA per (Y matrix, 256-row tile); thread = rows t and t + 128.
 // The tile's part of Y (256 consecutive rows of a row-major matrix) is produced
-// in column windows of 128 bytes (32 FP32 / 16 FP64 columns): every neutron
-// density sub-block (Q_l, Q_r) overlapping the window adds
+// in column windows of at most 128 bytes (32 FP32 / 16 FP64 columns).  A window
+// holds whole neutron density sub-blocks (Q_l, Q_r); a sub-block wider than the
+// window is cut at multiples of 8 outputs.  For each piece and each group of 8
+// outputs the thread accumulates
 //   Y[row, Q_l cols] = C[row, Q_r cols] rho^T
-// into a padded shared-memory tile, the row's C values held in registers (up to 8
-// per chunk, coalesced loads) and the density values read as warp-uniform 16-byte
-// loads (4 outputs x 2 rows = 8 FMAs per coefficient).  The window is then written
-// out with coalesced row segments and cleared in the same pass.  Every element of
-// Y is written, so Y needs no clearing between products.
+// over all nr coefficients in registers (C loads coalesced across the warp,
+// density values as warp-uniform 16-byte loads: 16 FMAs per 2 C values and 8
+// coefficients) and stores the result once into a padded shared-memory tile.  The
+// window is then written out as coalesced row segments, columns no sub-block
+// reaches as zeros, and cleared.  Every element of Y is written, so Y needs no
+// clearing between products.  A warp whose second (or both) 32-row slots lie past
+// the end of the matrix takes the one-row path (or only joins the barriers).
 template <typename T> struct KyWin;
 template <> struct KyWin<float> { static constexpr int W = 32; };
 template <> struct KyWin<double> { static constexpr int W = 16; };
 
-__device__ __forceinline__ void ky_load4(const float *p, float v[4]) {
-  const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
-  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+__device__ __forceinline__ void ky_load8(const float *p, float v[8]) {
+  const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+  const float4 b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
 }
-__device__ __forceinline__ void ky_load4(const double *p, double v[4]) {
-  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
-  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
-  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+__device__ __forceinline__ void ky_load8(const double *p, double v[8]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p) + i);
+    v[2 * i] = a.x;
+    v[2 * i + 1] = a.y;
+  }
 }
 
-// Adds the contribution of density columns [k0, k0 + KC) of one sub-block to the
-// tile columns of outputs l in [lo, hi) (relative to the sub-block), for both rows.
-template <typename T, int KC>
-__device__ __forceinline__ void ky_chunk(const T *__restrict__ c0p, const T *__restrict__ c1p, bool ok0, bool ok1,
-                                         int64_t m, const T *__restrict__ R, int ldr, int lo, int hi, T *t0, T *t1) {
-  T c0[KC], c1[KC];
+// Outputs l in [plo, phi) of one sub-block (plo a multiple of 8) for R rows of the
+// thread: c0 points at C[row, Q_r col 0] of the first row; rows are 128 apart in C
+// and 128 tile rows apart in t (t points at the tile column of output 0).
+template <typename T, int R>
+__device__ __forceinline__ void ky_piece(const T *__restrict__ c0, bool ok0, bool ok1, int64_t m,
+                                         const T *__restrict__ rb, int ldr, int nr, int plo, int phi, T *t,
+                                         int tstride) {
+  for (int g = plo; g < phi; g += 8) {
+    T a[R][8];
 #pragma unroll
-  for (int j = 0; j < KC; ++j) {
-    c0[j] = ok0 ? c0p[m * j] : T(0);
-    c1[j] = ok1 ? c1p[m * j] : T(0);
-  }
-  for (int g = lo & ~3; g < hi; g += 4) {
-    T a0[4] = {T(0), T(0), T(0), T(0)}, a1[4] = {T(0), T(0), T(0), T(0)};
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int j = 0; j < KC; ++j) {
-      T v[4];
-      ky_load4(R + (int64_t)ldr * j + g, v);
+      for (int q = 0; q < 8; ++q) a[r][q] = T(0);
+    const T *cp = c0;
+    const T *rp = rb + g;
+#pragma unroll 2
+    for (int k = 0; k < nr; ++k) {
+      T c[R];
+      c[0] = ok0 ? cp[0] : T(0);
+      if (R == 2) c[R - 1] = ok1 ? cp[128] : T(0);
+      T v[8];
+      ky_load8(rp, v);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a0[q] = fma(c0[j], v[q], a0[q]);
-        a1[q] = fma(c1[j], v[q], a1[q]);
-      }
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r][q] = fma(c[r], v[q], a[r][q]);
+      cp += m;
+      rp += ldr;
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int l = g + q;
-      if (l >= lo && l < hi) {
-        t0[l] += a0[q];
-        t1[l] += a1[q];
+    for (int q = 0; q < 8; ++q)
+      if (g + q < phi) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[r * tstride + g + q] = a[r][q];
       }
-    }
   }
 }
 
@@ -152,52 +165,50 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
   __shared__ T tile[KY_TILE_ROWS * LD];
   const YGroup g = groups[blockIdx.x];
   const int tid = threadIdx.x;
-  const int r0 = g.row0 + tid, r1 = r0 + 128;
-  const bool ok0 = r0 < g.m, ok1 = r1 < g.m;
+  const int rows = min(KY_TILE_ROWS, g.m - g.row0);
+  const int wrow = tid & ~31;                 // first tile row of the warp's first slot
+  const int mode = (wrow + 128 < rows) ? 2 : (wrow < rows ? 1 : 0);
+  const bool ok0 = tid < rows, ok1 = tid + 128 < rows;
   const int64_t m = g.m;
-  const T *C = x + g.c_base;
+  const T *C = x + g.c_base + g.row0 + tid;
   for (int e = tid; e < KY_TILE_ROWS * LD; e += 128) tile[e] = T(0);
   __syncthreads();
-  const int rows = min(KY_TILE_ROWS, g.m - g.row0);
   T *Yt = Y + g.y_base + (int64_t)g.row0 * g.ldy;
-  int bi = g.b_begin;
-  for (int w0 = 0; w0 < g.ldy; w0 += W) {
-    const int w1 = min(w0 + W, g.ldy);
-    while (bi < g.b_end && blks[bi].ycol + blks[bi].nl <= w0) ++bi;
-    for (int bj = bi; bj < g.b_end; ++bj) {
-      const YBlk b = blks[bj];
-      if (b.ycol >= w1) break;
-      const int lo = max(0, w0 - b.ycol), hi = min(b.nl, w1 - b.ycol);
-      // tile column of output l is b.ycol + l - w0
-      T *t0 = tile + tid * LD + (b.ycol - w0);
-      T *t1 = tile + (tid + 128) * LD + (b.ycol - w0);
-      const T *cb0 = C + r0 + m * b.ccol, *cb1 = C + r1 + m * b.ccol;
-      const T *R = rho + b.rho;
-      for (int k0 = 0; k0 < b.nr; k0 += 8) {
-        const int kc = min(8, b.nr - k0);
-        const T *c0p = cb0 + m * k0, *c1p = cb1 + m * k0;
-        const T *Rk = R + (int64_t)b.ldr * k0;
-        switch (kc) {
-          case 1: ky_chunk<T, 1>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 2: ky_chunk<T, 2>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 3: ky_chunk<T, 3>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 4: ky_chunk<T, 4>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 5: ky_chunk<T, 5>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 6: ky_chunk<T, 6>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          case 7: ky_chunk<T, 7>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-          default: ky_chunk<T, 8>(c0p, c1p, ok0, ok1, m, Rk, b.ldr, lo, hi, t0, t1); break;
-        }
+  const int fc = tid % W;                     // flush: column of this thread, rows fr, fr + 128/W, ...
+  int bi = g.b_begin, lst = 0;                // next sub-block and its first output not yet produced
+  int ws = 0;
+  while (ws < g.ldy) {
+    int we = min(ws + W, g.ldy);
+    int nbi = g.b_end, nlst = 0;
+    for (int j = bi, l0 = lst; j < g.b_end; ++j, l0 = 0) {
+      const YBlk b = blks[j];
+      const int bs = b.ycol + l0;
+      if (bs >= we) { nbi = j; nlst = l0; break; }
+      int hi = b.nl;
+      if (b.ycol + b.nl > we) {
+        if (l0 == 0 && b.ycol > ws) { we = b.ycol; nbi = j; nlst = 0; break; }  // next window starts here
+        hi = l0 + (we - bs);                                                     // cut: a multiple of 8
+        nbi = j;
+        nlst = hi;
       }
+      T *t = tile + tid * LD + (b.ycol - ws);
+      const T *c0 = C + m * b.ccol;
+      if (mode == 2) ky_piece<T, 2>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
+      else if (mode == 1) ky_piece<T, 1>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
+      if (hi < b.nl) break;
     }
     __syncthreads();
-    const int wn = w1 - w0;
-    for (int e = tid; e < rows * W; e += 128) {
-      const int r = e / W, c = e - r * W;
-      T *tp = tile + r * LD + c;
-      if (c < wn) Yt[(int64_t)r * g.ldy + w0 + c] = *tp;
+    const int wn = we - ws;
+    T *yp = Yt + ws + fc;
+    for (int r = tid / W; r < rows; r += 128 / W) {
+      T *tp = tile + r * LD + fc;
+      if (fc < wn) yp[(int64_t)r * g.ldy] = *tp;
       *tp = T(0);
     }
     __syncthreads();
+    ws = we;
+    bi = nbi;
+    lst = nlst;
   }
 }
 

@@ -55,11 +55,11 @@ struct Block {
 
 // ---- task lists of the H.v kernels -------------------------------------------
 // Y stage: Y_(h,b) = C_h * rho_b^T (row-major d_ar x d_bl), one group per (Y matrix, row tile).
-// The densities are re-laid out for it: every sub-block starts at a multiple of 4 elements and
-// has its leading dimension rounded up to a multiple of 4 (zero padding), so that groups of 4
-// outputs load their coefficients with 16-byte vector loads in FP32 and FP64.
+// The densities are re-laid out for it: every sub-block starts at a multiple of 8 elements and
+// has its leading dimension rounded up to a multiple of 8 (zero padding), so that groups of 8
+// outputs load their coefficients with aligned 16-byte vector loads in FP32 and FP64.
 constexpr int KY_TILE_ROWS = 256;  // 128 threads x 2 rows
-constexpr int KY_PAD = 4;
+constexpr int KY_PAD = 8;
 constexpr int KA_K_SPLIT = 512;   // stacked rows per k_a tile (longer slabs are split, partial sums added atomically)
 struct YGroup {
   int64_t c_base;   // element offset of input block h
