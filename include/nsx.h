@@ -127,6 +127,18 @@ typedef struct nsx_files {
 
 int nsx_load_files(const nsx_files *files, int device, nsx_handle **out);
 
+/* Replace the interaction of a handle without re-planning: new pn multipole values
+ * (op_vals, same count and order as nsx_problem.op_keys at creation, renorm applied as
+ * then) and new like-particle segment values (same segments and order as the
+ * nsx_species seg_vals at creation, a_nvals / b_nvals values).  The densities, the
+ * block structure and every buffer stay as they are; the call copies the new operands
+ * to the device synchronously and allocates nothing.  The reference re-runs NuOp and
+ * reloads its files for a new interaction (src/NuLnz/NuCoreX.f90:1133-1142 reads the
+ * .oph values, 1216-1319 the .mat segments); this is that reload for a handle already
+ * in memory, used by interaction sweeps. */
+int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals,
+                        int64_t a_nvals, const double *b_seg_vals, int64_t b_nvals);
+
 /* The 3-character NuShellX file code (src/NuCommon/NuModules.F90:22-35). */
 int nsx_file_code(int32_t i, int32_t j, int32_t k, char out[4]);
 
@@ -181,6 +193,33 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out);
 
 void nsx_destroy(nsx_handle *h);
 const char *nsx_last_error(void);
+
+/* ---- Learned start vector: the network --------------------------------------
+ * No counterpart in the reference, whose start vector is always the seeded random
+ * one (src/NuLnz/NuCoreX.f90:625-654).  A 3-layer MLP n_in -> width -> width -> n_out
+ * with SiLU, FP32 weights and BF16 hidden activations, trained (full-batch Adam on a
+ * mean-squared error) and evaluated by the library's own CUDA kernels.  It maps the
+ * coefficients of an interaction variant to the compressed ground state (weights on
+ * the dominant proton x neutron sub-blocks) from which the host builds the start
+ * vector passed to nsx_solve.  Parameters are one flat FP32 array:
+ * W1[width][n_in], b1[width], W2[width][width], b2[width], W3[n_out][width], b3[n_out].
+ * Inputs x are [batch][n_in], targets and outputs [batch][n_out], all FP32 host
+ * arrays.  Errors: negative NSX_E_* codes with nsx_mlp_last_error(). */
+typedef struct nsx_mlp nsx_mlp;
+int nsx_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64_t seed, int device, nsx_mlp **out);
+int64_t nsx_mlp_param_count(const nsx_mlp *net);
+int nsx_mlp_set_params(nsx_mlp *net, const float *params, int64_t n);  /* also resets Adam */
+int nsx_mlp_get_params(const nsx_mlp *net, float *params, int64_t n);
+/* y = net(x) */
+int nsx_mlp_forward(nsx_mlp *net, const float *x, int32_t batch, float *y);
+/* loss = mean (net(x) - t)^2 over batch x n_out, and its gradient w.r.t. the
+ * parameters (grad may be NULL; the gradient stays on the device for nsx_mlp_train) */
+int nsx_mlp_gradients(nsx_mlp *net, const float *x, const float *t, int32_t batch, float *loss, float *grad);
+/* steps of full-batch Adam (beta 0.9 / 0.999, eps 1e-8) at learning rate lr on the
+ * batch (uploaded once); loss = the loss after the last step */
+int nsx_mlp_train(nsx_mlp *net, const float *x, const float *t, int32_t batch, int32_t steps, float lr, float *loss);
+void nsx_mlp_destroy(nsx_mlp *net);
+const char *nsx_mlp_last_error(void);
 
 #ifdef __cplusplus
 }

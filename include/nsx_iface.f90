@@ -80,6 +80,14 @@ module nsx_iface
        integer(c_int), value :: device
        type(c_ptr), intent(out) :: out
      end function
+     integer(c_int) function nsx_set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals) &
+          bind(C, name="nsx_set_interaction")
+       import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: op_vals(*), a_seg_vals(*), b_seg_vals(*)
+       integer(c_int32_t), value :: nop
+       integer(c_int64_t), value :: a_nvals, b_nvals
+     end function
      integer(c_int) function nsx_file_code(i, j, k, code) bind(C, name="nsx_file_code")
        import :: c_int, c_int32_t, c_char
        integer(c_int32_t), value :: i, j, k
@@ -147,6 +155,60 @@ module nsx_iface
        type(c_ptr), value :: h
      end subroutine
      type(c_ptr) function nsx_last_error() bind(C, name="nsx_last_error")
+       import :: c_ptr
+     end function
+     ! ---- learned start vector: the network (nsx_mlp_*) ----
+     integer(c_int) function nsx_mlp_create(n_in, width, n_out, seed, device, net) bind(C, name="nsx_mlp_create")
+       import :: c_int, c_int32_t, c_int64_t, c_ptr
+       integer(c_int32_t), value :: n_in, width, n_out
+       integer(c_int64_t), value :: seed
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: net
+     end function
+     integer(c_int64_t) function nsx_mlp_param_count(net) bind(C, name="nsx_mlp_param_count")
+       import :: c_int64_t, c_ptr
+       type(c_ptr), value :: net
+     end function
+     integer(c_int) function nsx_mlp_set_params(net, params, n) bind(C, name="nsx_mlp_set_params")
+       import :: c_int, c_int64_t, c_float, c_ptr
+       type(c_ptr), value :: net
+       real(c_float), intent(in) :: params(*)
+       integer(c_int64_t), value :: n
+     end function
+     integer(c_int) function nsx_mlp_get_params(net, params, n) bind(C, name="nsx_mlp_get_params")
+       import :: c_int, c_int64_t, c_float, c_ptr
+       type(c_ptr), value :: net
+       real(c_float), intent(out) :: params(*)
+       integer(c_int64_t), value :: n
+     end function
+     integer(c_int) function nsx_mlp_forward(net, x, batch, y) bind(C, name="nsx_mlp_forward")
+       import :: c_int, c_int32_t, c_float, c_ptr
+       type(c_ptr), value :: net
+       real(c_float), intent(in) :: x(*)
+       integer(c_int32_t), value :: batch
+       real(c_float), intent(out) :: y(*)
+     end function
+     integer(c_int) function nsx_mlp_gradients(net, x, t, batch, loss, grad) bind(C, name="nsx_mlp_gradients")
+       import :: c_int, c_int32_t, c_float, c_ptr
+       type(c_ptr), value :: net
+       real(c_float), intent(in) :: x(*), t(*)
+       integer(c_int32_t), value :: batch
+       real(c_float), intent(out) :: loss
+       type(c_ptr), value :: grad                      ! c_loc(g(1)) or c_null_ptr
+     end function
+     integer(c_int) function nsx_mlp_train(net, x, t, batch, steps, lr, loss) bind(C, name="nsx_mlp_train")
+       import :: c_int, c_int32_t, c_float, c_ptr
+       type(c_ptr), value :: net
+       real(c_float), intent(in) :: x(*), t(*)
+       integer(c_int32_t), value :: batch, steps
+       real(c_float), value :: lr
+       real(c_float), intent(out) :: loss
+     end function
+     subroutine nsx_mlp_destroy(net) bind(C, name="nsx_mlp_destroy")
+       import :: c_ptr
+       type(c_ptr), value :: net
+     end subroutine
+     type(c_ptr) function nsx_mlp_last_error() bind(C, name="nsx_mlp_last_error")
        import :: c_ptr
      end function
   end interface

@@ -85,6 +85,15 @@ int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
   return nsx_create(&p, device, out);
 }
 
+int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
+                        const double *b_seg_vals, int64_t b_nvals) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals);
+    upload_interaction(h);
+  });
+}
+
 int64_t nsx_dim(const nsx_handle *h) { return h ? h->no_state : 0; }
 int32_t nsx_nblocks(const nsx_handle *h) { return h ? (int32_t)h->blocks.size() : 0; }
 

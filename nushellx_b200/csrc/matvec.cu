@@ -380,6 +380,30 @@ static S *dev_copy_pod(const std::vector<S> &v) {
 
 static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
+template <typename T>
+static void dev_refill(T *p, const std::vector<double> &v) {
+  if (v.empty() || !p) return;
+  std::vector<T> tmp(v.begin(), v.end());
+  NSX_CUDA(cudaMemcpy(p, tmp.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+// Copies the interaction-dependent operands (mixing weights, dense like-particle H) into the
+// device buffers the handle already holds, in every precision that has been set up.  The
+// copies are synchronous, so products issued afterwards on any stream see the new values.
+void upload_interaction(nsx_handle *h) {
+  NSX_CUDA(cudaSetDevice(h->device));
+  NSX_CUDA(cudaDeviceSynchronize());  // no product of the old interaction may still read them
+  auto &d = h->d;
+  dev_refill<double>(d.w, h->weights);
+  dev_refill<double>(d.hA, h->A.hdense);
+  dev_refill<double>(d.hB, h->B.hdense);
+  if (d.w32) {
+    dev_refill<float>(d.w32, h->weights);
+    dev_refill<float>(d.hA32, h->A.hdense);
+    dev_refill<float>(d.hB32, h->B.hdense);
+  }
+}
+
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
   if (h->max_anl > 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");

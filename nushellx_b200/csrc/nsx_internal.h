@@ -35,9 +35,12 @@ struct SpeciesPlan {
   std::unordered_map<uint64_t, int> key_index;
   std::vector<std::vector<RhoBlk>> kblocks;  // per key
   std::vector<double> vals;           // all density values (.trd order)
-  // like-particle Hamiltonian, dense per J (d x d, column-major, symmetric)
+  // like-particle Hamiltonian, dense per J (d x d, column-major, symmetric), and the layout of
+  // the .mat segments it was built from (kept so that new segment values can replace it)
   std::vector<int64_t> hoff;          // [nJ+1] offsets into hdense
   std::vector<double> hdense;
+  std::vector<int> seg_J2, seg_np, seg_npr;
+  std::vector<int64_t> seg_off;
 
   int jidx(int J2) const { return (J2 - minJ2) / 2; }
   bool has_J(int J2) const { return J2 >= minJ2 && J2 <= maxJ2 && ((J2 - minJ2) % 2 == 0); }
@@ -51,6 +54,14 @@ uint64_t pack_key(int b0, int b1, int b2, int b3, int b4);
 struct Block {
   int J2a, J2b, da, db;
   int64_t off;
+};
+
+// One term of a mixing weight: weights[w] += V(op) * rw, V the multipole value of operator
+// op (its index in the problem's op list, renorm applied) and rw the Racah factor.
+struct WTerm {
+  int64_t w;
+  int32_t op;
+  double rw;
 };
 
 // ---- task lists of the H.v kernels -------------------------------------------
@@ -152,8 +163,12 @@ struct nsx_handle {
   int64_t no_state = 0;
   std::vector<uint8_t> lcoef;
   double renorm = 1.0;
-  // pn multipole interaction: key (sal, sar, sbl, sbr, lam) -> V * renorm
+  // pn multipole interaction: key (sal, sar, sbl, sbr, lam) -> V * renorm, and -> index in the
+  // op list of the problem the handle was created from
   std::unordered_map<uint64_t, double> vop;
+  std::unordered_map<uint64_t, int> vop_index;
+  int nop = 0;
+  std::vector<nsx::WTerm> wterms;  // every weight as a sum of (V, Racah factor) terms, in summation order
   // plan
   std::vector<nsx::YGroup> ygroups;
   std::vector<nsx::YBlk> yblks;
@@ -182,7 +197,10 @@ struct nsx_handle {
 
 namespace nsx {
 void build_plan(nsx_handle *h, const nsx_problem *p);
+void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
+                     const double *b_seg_vals, int64_t b_nvals);
 void upload(nsx_handle *h);
+void upload_interaction(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);

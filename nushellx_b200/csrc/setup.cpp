@@ -67,6 +67,8 @@ static double racah_weight(int Jal, int Jbl, int Jar, int Jbr, int J, int lam) {
 }
 
 // ---- species ------------------------------------------------------------------
+static void fill_hdense(SpeciesPlan &S, const double *seg_vals);
+
 static void load_species(SpeciesPlan &S, const nsx_species &s, const char *name) {
   if (s.nspart <= 0 || s.maxJ2 < s.minJ2 || ((s.maxJ2 - s.minJ2) % 2) != 0)
     fail(NSX_E_ARG, std::string("species ") + name + ": bad partition count or J range");
@@ -113,19 +115,34 @@ static void load_species(SpeciesPlan &S, const nsx_species &s, const char *name)
     int64_t d = S.poff[j][S.nspart];
     S.hoff[j + 1] = S.hoff[j] + d * d;
   }
-  S.hdense.assign(S.hoff[S.nJ], 0.0);
+  S.seg_J2.assign(s.seg_J2, s.seg_J2 + s.nseg);
+  S.seg_np.assign(s.seg_np, s.seg_np + s.nseg);
+  S.seg_npr.assign(s.seg_npr, s.seg_npr + s.nseg);
+  S.seg_off.assign(s.seg_off, s.seg_off + s.nseg + 1);
   for (int g = 0; g < s.nseg; ++g) {
-    int J2 = s.seg_J2[g];
+    int J2 = S.seg_J2[g];
     if (!S.has_J(J2)) fail(NSX_E_ARG, std::string("species ") + name + ": segment J out of range");
-    int j = S.jidx(J2);
-    int np = s.seg_np[g] - 1, npr = s.seg_npr[g] - 1;
+    int np = S.seg_np[g] - 1, npr = S.seg_npr[g] - 1;
     if (np < 0 || npr < 0 || np >= S.nspart || npr >= S.nspart || npr < np)
       fail(NSX_E_ARG, std::string("species ") + name + ": bad segment partitions");
     int nl = S.njt_of(np, J2), nr = S.njt_of(npr, J2);
-    if ((int64_t)nl * nr != s.seg_off[g + 1] - s.seg_off[g]) fail(NSX_E_ARG, std::string("species ") + name + ": segment size mismatch");
+    if ((int64_t)nl * nr != S.seg_off[g + 1] - S.seg_off[g])
+      fail(NSX_E_ARG, std::string("species ") + name + ": segment size mismatch");
+  }
+  fill_hdense(S, s.seg_vals);
+}
+
+// Dense like-particle H per J from segment values laid out as recorded by load_species.
+static void fill_hdense(SpeciesPlan &S, const double *seg_vals) {
+  S.hdense.assign(S.hoff[S.nJ], 0.0);
+  for (size_t g = 0; g < S.seg_J2.size(); ++g) {
+    int J2 = S.seg_J2[g];
+    int j = S.jidx(J2);
+    int np = S.seg_np[g] - 1, npr = S.seg_npr[g] - 1;
+    int nl = S.njt_of(np, J2), nr = S.njt_of(npr, J2);
     int64_t d = S.poff[j][S.nspart];
     double *H = S.hdense.data() + S.hoff[j];
-    const double *M = s.seg_vals + s.seg_off[g];
+    const double *M = seg_vals + S.seg_off[g];
     int ro = S.poff[j][np], co = S.poff[j][npr];
     // matrix(dimptr, dimpt): value[kr + nr*kl] = H[(np,kl), (npr,kr)]
     for (int kl = 0; kl < nl; ++kl)
@@ -137,6 +154,31 @@ static void load_species(SpeciesPlan &S, const nsx_species &s, const char *name)
   }
 }
 
+void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
+                     const double *b_seg_vals, int64_t b_nvals) {
+  if (nop != h->nop) fail(NSX_E_ARG, "op_vals holds " + std::to_string(nop) + " values; the handle was created with " +
+                                         std::to_string(h->nop) + " operators");
+  if (nop > 0 && !op_vals) fail(NSX_E_ARG, "null op_vals");
+  const int64_t na = h->A.seg_off.empty() ? 0 : h->A.seg_off.back();
+  const int64_t nb = h->B.seg_off.empty() ? 0 : h->B.seg_off.back();
+  if (a_nvals != na || b_nvals != nb)
+    fail(NSX_E_ARG, "segment value counts " + std::to_string(a_nvals) + ", " + std::to_string(b_nvals) +
+                        " differ from the handle's " + std::to_string(na) + ", " + std::to_string(nb));
+  if ((na > 0 && !a_seg_vals) || (nb > 0 && !b_seg_vals)) fail(NSX_E_ARG, "null segment values");
+  std::vector<double> v(nop);
+  for (int i = 0; i < nop; ++i) {
+    double x = op_vals[i];
+    if (!std::isfinite(x)) fail(NSX_E_ARG, "op_vals holds a value that is not finite");
+    if (std::fabs(x) < 1e-10) x = 0.0;
+    v[i] = x * h->renorm;
+  }
+  for (auto &kv : h->vop_index) h->vop[kv.first] = v[kv.second];
+  std::fill(h->weights.begin(), h->weights.end(), 0.0);
+  for (const WTerm &t : h->wterms) h->weights[t.w] += v[t.op] * t.rw;
+  fill_hdense(h->A, a_seg_vals);
+  fill_hdense(h->B, b_seg_vals);
+}
+
 void build_plan(nsx_handle *h, const nsx_problem *p) {
   h->J2 = p->J2;
   h->parity = p->parity;
@@ -145,11 +187,14 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   load_species(h->B, p->b, "b");
   SpeciesPlan &A = h->A, &B = h->B;
   // pn multipole interaction (src/NuLnz/NuCoreX.f90:1133-1142: tiny values zeroed, times renorm)
+  h->nop = p->nop;
   for (int i = 0; i < p->nop; ++i) {
     const uint8_t *kb = p->op_keys + 8 * (size_t)i;
     double v = p->op_vals[i];
     if (std::fabs(v) < 1e-10) v = 0.0;
-    h->vop[pack_key(kb[0], kb[1], kb[2], kb[3], kb[4])] = v * p->renorm;
+    const uint64_t key = pack_key(kb[0], kb[1], kb[2], kb[3], kb[4]);
+    h->vop[key] = v * p->renorm;
+    h->vop_index[key] = i;
   }
   // block list (src/NuLnz/NuCoreX.f90:926-988): ascending (2Ja, 2Jb)
   const int J2 = p->J2;
@@ -214,7 +259,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
 
   // ---- pn table (drdbh, src/NuLnz/NuCoreX.f90:1428-1577) ----------------------
   // Rows: (output block, J_ar, proton density key a) with entries (neutron key b, input block h, weight).
-  struct Entry { int bk, hb; double w; };
+  struct Entry { int bk, hb; double w; int op; double rw; };
   struct Row { int bl, jar, ak, lam; std::vector<Entry> e; };
   std::vector<Row> table;
   for (size_t bl = 0; bl < h->blocks.size(); ++bl) {
@@ -243,10 +288,13 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           for (int bk : bit->second) {
             uint64_t bkey = B.keys[bk];
             int sbl = (bkey >> 16) & 255, sbr = (bkey >> 24) & 255;
-            auto vit = h->vop.find(pack_key(sal, sar, sbl, sbr, lam));
-            if (vit == h->vop.end() || vit->second == 0.0) continue;
+            // operators of the problem's list are kept even where V is zero, so that a new
+            // interaction (nsx_set_interaction) finds a slot for every one of them
+            const uint64_t okey = pack_key(sal, sar, sbl, sbr, lam);
+            auto vit = h->vop.find(okey);
+            if (vit == h->vop.end()) continue;
             if (B.kblocks[bk].empty()) continue;
-            row.e.push_back({bk, hit->second, vit->second * rw});
+            row.e.push_back({bk, hit->second, vit->second * rw, h->vop_index[okey], rw});
           }
         }
         if (!row.e.empty()) table.push_back(std::move(row));
@@ -370,6 +418,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           int si = sidx[{e.hb, e.bk}];
           if (si >= (int)s0 && si < (int)s1) {
             wr[si - s0] += e.w;
+            h->wterms.push_back({(int64_t)G.w_off + (int64_t)ai * G.ns + (si - (int)s0), e.op, e.rw});
             active[ai] = 1;
           }
         }

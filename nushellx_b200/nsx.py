@@ -77,6 +77,8 @@ SYMBOLS = {
     "nsx_create": (C.c_int, [_p(Problem), C.c_int, _p(C.c_void_p)]),
     "nsx_load_files": (C.c_int, [_p(Files), C.c_int, _p(C.c_void_p)]),
     "nsx_file_code": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p]),
+    "nsx_set_interaction": (C.c_int, [C.c_void_p, _p(C.c_double), C.c_int32, _p(C.c_double), C.c_int64,
+                                      _p(C.c_double), C.c_int64]),
     "nsx_dim": (C.c_int64, [C.c_void_p]),
     "nsx_nblocks": (C.c_int32, [C.c_void_p]),
     "nsx_blocks": (C.c_int, [C.c_void_p, _p(C.c_int32), _p(C.c_int64)]),
@@ -90,6 +92,17 @@ SYMBOLS = {
     "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
     "nsx_destroy": (None, [C.c_void_p]),
     "nsx_last_error": (C.c_char_p, []),
+    "nsx_mlp_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int, _p(C.c_void_p)]),
+    "nsx_mlp_param_count": (C.c_int64, [C.c_void_p]),
+    "nsx_mlp_set_params": (C.c_int, [C.c_void_p, _p(C.c_float), C.c_int64]),
+    "nsx_mlp_get_params": (C.c_int, [C.c_void_p, _p(C.c_float), C.c_int64]),
+    "nsx_mlp_forward": (C.c_int, [C.c_void_p, _p(C.c_float), C.c_int32, _p(C.c_float)]),
+    "nsx_mlp_gradients": (C.c_int, [C.c_void_p, _p(C.c_float), _p(C.c_float), C.c_int32, _p(C.c_float),
+                                    _p(C.c_float)]),
+    "nsx_mlp_train": (C.c_int, [C.c_void_p, _p(C.c_float), _p(C.c_float), C.c_int32, C.c_int32, C.c_float,
+                                _p(C.c_float)]),
+    "nsx_mlp_destroy": (None, [C.c_void_p]),
+    "nsx_mlp_last_error": (C.c_char_p, []),
 }
 
 _lib = None
@@ -159,6 +172,16 @@ def _species_struct(keep, S, dens, segs):
     return s
 
 
+def op_order(vlam):
+    """The order of the pn multipole operators in nsx_problem.op_keys (sorted labels)."""
+    return sorted(vlam)
+
+
+def op_values(vlam, order):
+    """Multipole values in a given operator order (0 for labels the dict does not hold)."""
+    return np.array([vlam.get(k, 0.0) for k in order], dtype=np.float64)
+
+
 def build_problem_struct(P):
     """nsx_problem for an in-memory generated problem; returns (struct, arrays to keep alive)."""
     from .gen.writer import density_arrays, segment_arrays
@@ -168,14 +191,13 @@ def build_problem_struct(P):
     prob.a = _species_struct(keep, P.A, density_arrays(P.A, P.rhoA), segment_arrays(P.A, P.segA))
     prob.b = _species_struct(keep, P.B, density_arrays(P.B, P.rhoB), segment_arrays(P.B, P.segB))
     norb = P.space.norb
-    okeys, ovals = [], []
-    for (o1, o3, o2, o4, lam), v in sorted(P.vlam.items()):
+    okeys = []
+    for (o1, o3, o2, o4, lam) in op_order(P.vlam):
         okeys.append(bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]))
-        ovals.append(v)
     ok = np.frombuffer(b"".join(okeys), dtype=np.uint8).copy()
-    ov = np.array(ovals, dtype=np.float64)
+    ov = op_values(P.vlam, op_order(P.vlam))
     keep.append((ok, ov))
-    prob.nop = len(ovals)
+    prob.nop = len(ov)
     prob.op_keys = _ptr(ok, C.c_uint8)
     prob.op_vals = _ptr(ov, C.c_double)
     prob.renorm = P.renorm
@@ -245,6 +267,16 @@ class Solver:
         _check(self._lib.nsx_matvec(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), precision,
                                     C.c_void_p(stream) if stream else None))
 
+    def set_interaction(self, op_vals, a_seg_vals, b_seg_vals):
+        """New pn multipole values (order of the creating problem's op keys) and like-particle
+        segment values for this handle, without re-planning (nsx_set_interaction)."""
+        ov = np.ascontiguousarray(op_vals, dtype=np.float64)
+        av = np.ascontiguousarray(a_seg_vals, dtype=np.float64)
+        bv = np.ascontiguousarray(b_seg_vals, dtype=np.float64)
+        _check(self._lib.nsx_set_interaction(self._h, ov.ctypes.data_as(_p(C.c_double)), len(ov),
+                                             av.ctypes.data_as(_p(C.c_double)), len(av),
+                                             bv.ctypes.data_as(_p(C.c_double)), len(bv)))
+
     def matvec_noalloc(self, x_ptr, y_ptr, stream=None):
         """FP64 H.v with the fixed device scratch array (no allocation in the call)."""
         _check(self._lib.nsx_matvec_noalloc(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
@@ -280,6 +312,71 @@ class Solver:
     def close(self):
         if self._h:
             self._lib.nsx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _mcheck(rc):
+    if rc != 0:
+        raise NsxError(rc, _lib.nsx_mlp_last_error().decode(errors="replace"))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Network:
+    """The learned start vector's MLP on a GPU (nsx_mlp_*): n_in -> width -> width -> n_out."""
+
+    def __init__(self, n_in, width, n_out, seed=1, device=0):
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        _mcheck(self._lib.nsx_mlp_create(n_in, width, n_out, seed, device, C.byref(self._h)))
+        self.n_in, self.width, self.n_out = n_in, width, n_out
+        self.nparams = int(self._lib.nsx_mlp_param_count(self._h))
+
+    @property
+    def params(self):
+        p = np.zeros(self.nparams, dtype=np.float32)
+        _mcheck(self._lib.nsx_mlp_get_params(self._h, p.ctypes.data_as(_p(C.c_float)), self.nparams))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p)
+        _mcheck(self._lib.nsx_mlp_set_params(self._h, p.ctypes.data_as(_p(C.c_float)), len(p)))
+
+    def forward(self, x):
+        x = _f32(x).reshape(-1, self.n_in)
+        y = np.zeros((len(x), self.n_out), dtype=np.float32)
+        _mcheck(self._lib.nsx_mlp_forward(self._h, x.ctypes.data_as(_p(C.c_float)), len(x),
+                                          y.ctypes.data_as(_p(C.c_float))))
+        return y
+
+    def gradients(self, x, t):
+        x, t = _f32(x).reshape(-1, self.n_in), _f32(t).reshape(-1, self.n_out)
+        loss = C.c_float()
+        g = np.zeros(self.nparams, dtype=np.float32)
+        _mcheck(self._lib.nsx_mlp_gradients(self._h, x.ctypes.data_as(_p(C.c_float)),
+                                            t.ctypes.data_as(_p(C.c_float)), len(x), C.byref(loss),
+                                            g.ctypes.data_as(_p(C.c_float))))
+        return float(loss.value), g
+
+    def train(self, x, t, steps, lr):
+        x, t = _f32(x).reshape(-1, self.n_in), _f32(t).reshape(-1, self.n_out)
+        loss = C.c_float()
+        _mcheck(self._lib.nsx_mlp_train(self._h, x.ctypes.data_as(_p(C.c_float)), t.ctypes.data_as(_p(C.c_float)),
+                                        len(x), steps, lr, C.byref(loss)))
+        return float(loss.value)
+
+    def close(self):
+        if self._h:
+            self._lib.nsx_mlp_destroy(self._h)
             self._h = None
 
     def __del__(self):
