@@ -6,12 +6,15 @@ each) and columns over neutron partitions Q.  Sub-block (k, P, Q) is the nJT(P, 
 nJT(Q, Jb) piece of it; only pieces of the requested parity are kept (the others are
 zero in every eigenvector).
 
-Compression: the K sub-blocks on which a reference ground state g_ref has the most
-weight are kept, each with its unit shape u_s = g_ref|s / |g_ref|s|.  A ground state g
-is represented by its projections w_s = <g|s, u_s>, with the overall sign of g chosen so
-that the projections sum to a non-negative value (g_ref itself gives w_s = |g_ref|s| > 0);
-the vector sum_s w_s u_s restores g up to what lies outside the kept pieces and the change
-of shape within them.
+Compression: K sub-blocks are kept, each with a unit shape u_s, and a ground state g is
+represented by its projections w_s = <g|s, u_s>; the vector sum_s w_s u_s restores g up to
+what lies outside the kept pieces and the change of shape within them.  Two ways to choose
+them: from one reference state g_ref (its K heaviest sub-blocks, u_s = g_ref|s / |g_ref|s|),
+or from a training set of ground states (the K sub-blocks of largest mean weight; u_s the
+dominant left singular vector of the training restrictions g_v|s, which does not depend on
+the arbitrary overall sign of each g_v).  The overall sign of a compressed state is fixed
+on the first kept sub-block, in the order of decreasing mean weight, that holds at least a
+tenth of its largest projection: that projection is made positive.
 """
 import numpy as np
 
@@ -61,15 +64,44 @@ def element_index(desc):
 
 
 class Compressor:
-    def __init__(self, desc, shapes, dim):
+    def __init__(self, desc, shapes, dim, rank=None):
         """desc: [K, 4] kept sub-blocks (offset, ld, rows, cols); shapes: their unit shapes,
-        concatenated (rows fastest); dim: vector length."""
+        concatenated (rows fastest); dim: vector length; rank: the order of the kept
+        sub-blocks by decreasing weight (used for the sign convention; default: as given)."""
         self.desc = np.asarray(desc, dtype=np.int64).reshape(-1, 4)
         self.shapes = np.asarray(shapes, dtype=np.float64)
         self.dim = int(dim)
         self.index, self.start = element_index(self.desc)
         assert len(self.shapes) == len(self.index)
         self.lengths = np.diff(self.start)
+        self.rank = np.arange(len(self.desc)) if rank is None else np.asarray(rank, dtype=np.int64)
+
+    @classmethod
+    def from_training(cls, sub, G, K=256):
+        """G: training ground states [n, dim] (a torch tensor on the GPU or a numpy array)."""
+        import torch
+        Gt = torch.as_tensor(G)
+        e_elem = torch.zeros(Gt.shape[1], dtype=torch.float64, device=Gt.device)
+        for c in range(0, Gt.shape[0], 32):
+            e_elem += (Gt[c:c + 32].double() ** 2).sum(0)
+        e_elem = (e_elem / Gt.shape[0]).cpu().numpy()
+        e = np.add.reduceat(e_elem[sub.index], sub.start[:-1])   # mean weight per sub-block
+        order = np.argsort(-e, kind="stable")[:K]           # by decreasing mean weight
+        keep = np.sort(order)                                # stored in vector order
+        rank = np.searchsorted(keep, order)                  # positions of the ranked blocks in keep
+        desc = sub.desc[keep]
+        sidx, sstart = element_index(desc)
+        shapes = np.zeros(len(sidx))
+        for s in range(len(desc)):
+            cols = torch.as_tensor(sidx[sstart[s]:sstart[s + 1]], device=Gt.device)
+            M = Gt[:, cols].double().T                       # [n_s, n]
+            if M.shape[0] == 1:
+                u = torch.ones(1, dtype=torch.float64, device=Gt.device)
+            else:
+                U, S, _ = torch.linalg.svd(M, full_matrices=False)
+                u = U[:, 0]
+            shapes[sstart[s]:sstart[s + 1]] = u.cpu().numpy()
+        return cls(desc, shapes, sub.dim, rank)
 
     @classmethod
     def from_reference(cls, sub, g_ref, K=256):
@@ -79,7 +111,7 @@ class Compressor:
         idx, start = element_index(desc)
         u = np.asarray(g_ref, dtype=np.float64)[idx]
         u /= np.repeat(n[keep], np.diff(start))
-        return cls(desc, u, sub.dim)
+        return cls(desc, u, sub.dim, np.searchsorted(keep, np.argsort(-n, kind="stable")[:K]))
 
     @property
     def K(self):
@@ -88,7 +120,9 @@ class Compressor:
     def compress(self, g):
         gs = np.asarray(g, dtype=np.float64)[self.index]
         w = np.add.reduceat(gs * self.shapes, self.start[:-1])
-        return w if w.sum() >= 0 else -w
+        big = np.abs(w[self.rank]) >= 0.1 * np.abs(w).max()
+        lead = self.rank[int(np.argmax(big))]
+        return w if w[lead] >= 0 else -w
 
     def decompress(self, w):
         x = np.zeros(self.dim)

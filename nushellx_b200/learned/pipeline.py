@@ -7,16 +7,19 @@
 Sweep: variants TBME = base + sum_i lam_i P_i (lam ~ U[-0.3, 0.3]^8, seeded; gen.variants)
 of one workload.  One solver handle is planned once; every variant is loaded into it with
 nsx_set_interaction and its ground state is found by the solver itself (FP32 H.v, FP64
-Lanczos, FP64 Rayleigh-Ritz refinement).  The ground state of the base interaction fixes
-the K = 256 kept sub-blocks and their shapes (learned.compress); each variant's ground state
-is stored as its K projections.
+Lanczos, FP64 Rayleigh-Ritz refinement) and kept in HBM.  The training variants' ground
+states fix the K = 256 kept sub-blocks and their shapes (learned.compress); each variant's
+ground state is stored as its K projections.
 
 Training: the network (nsx_mlp, FP32 weights, BF16 activations, trained by libnsx's CUDA
 kernels) maps lam / 0.3 to the standardised projections; full-batch Adam.
 
-Start vector: the predicted projections, decompressed onto the kept sub-blocks, plus a
-small share (beta) of the standard seeded random vector so that every eigenvector has a
-component; the solve then starts from it without the power pre-iterations.  The standard
+Start vector: the predicted projections, decompressed onto the kept sub-blocks and
+normalised, plus beta (default 1) times the normalised standard seeded random vector, so
+that every eigenvector keeps a component comparable to the standard start's (a start that
+is almost only the ground state can let Lanczos meet its stopping test with one of the
+lowest states still missing); the solve then starts from it without the power
+pre-iterations.  The standard
 start vector remains the fallback (no model for the workload, or a dimension mismatch).
 """
 import argparse
@@ -52,36 +55,41 @@ def standard_start(S, seed=5):
     return np.random.default_rng(seed).uniform(-0.5, 0.5, S.dim) * S.lcoef
 
 
-def sweep(workload, nvar, seed, K, out, tol=1e-5, log=print):
+def sweep(workload, nvar, seed, K, out, ntrain=None, tol=1e-5, log=print):
+    """Ground states of nvar seeded variants; the compression is built from the first ntrain
+    of them (default: all) and every variant is stored as its K projections."""
+    import torch
     from .compress import SubBlocks, Compressor
     from ..gen.variants import sample_lambdas
+    ntrain = nvar if ntrain is None else ntrain
     t0 = time.time()
     P, fam, S = _solver_and_family(workload)
     log(f"setup {time.time() - t0:.1f} s, dim {S.dim}")
-    e_base, g_base, rep = ground_state(S, tol)
-    sub = SubBlocks(P)
-    comp = Compressor.from_reference(sub, g_base, K)
-    cap_base = float((comp.compress(g_base) ** 2).sum())
-    log(f"base E0 {e_base:.6f} MeV, {rep['iterations']} iterations; {len(sub)} sub-blocks, top {K} hold "
-        f"{cap_base:.4f} of |g|^2")
     lams = sample_lambdas(nvar, NPERTURB, seed, LAM_SCALE)
-    W = np.zeros((nvar, K))
+    G = torch.zeros((nvar, S.dim), dtype=torch.float32, device="cuda")   # ground states, kept in HBM
     E0 = np.zeros(nvar)
     iters = np.zeros(nvar, dtype=np.int64)
-    captured = np.zeros(nvar)
     t1 = time.time()
     for v in range(nvar):
         S.set_interaction(*fam.arrays(lams[v]))
         E0[v], g, rep = ground_state(S, tol)
-        W[v] = comp.compress(g)
-        captured[v] = float((W[v] ** 2).sum())
+        G[v] = torch.from_numpy(g.astype(np.float32)).to("cuda")
         iters[v] = rep["iterations"]
         if v % 32 == 0 or v == nvar - 1:
-            log(f"variant {v}: E0 {E0[v]:.5f} MeV, {iters[v]} iterations, captured {captured[v]:.3f}, "
-                f"{(time.time() - t1) / (v + 1):.2f} s per variant")
+            log(f"variant {v}: E0 {E0[v]:.5f} MeV, {iters[v]} iterations, {(time.time() - t1) / (v + 1):.2f} s per variant")
+    sub = SubBlocks(P)
+    comp = Compressor.from_training(sub, G[:ntrain], K)
+    W = np.zeros((nvar, K))
+    for v in range(nvar):
+        W[v] = comp.compress(G[v].double().cpu().numpy())
+    captured = (W ** 2).sum(1)
+    log(f"{len(sub)} sub-blocks; the {K} kept hold {captured[:ntrain].mean():.4f} of |g|^2 on average over the "
+        f"training variants (min {captured.min():.4f}), {captured[ntrain:].mean() if nvar > ntrain else float('nan'):.4f} "
+        f"over the others")
     np.savez(out, workload=workload, lams=lams, W=W, E0=E0, iterations=iters, captured=captured,
-             desc=comp.desc, shapes=comp.shapes.astype(np.float32), dim=S.dim, e_base=e_base,
+             desc=comp.desc, shapes=comp.shapes.astype(np.float32), rank=comp.rank, dim=S.dim, ntrain=ntrain,
              lam_scale=LAM_SCALE, perturb_seed0=PERTURB_SEED0, nperturb=NPERTURB, variant_seed=seed)
+    del G
     S.close()
     return out
 
@@ -106,7 +114,7 @@ def train(data, ntrain, out, width=256, steps=4000, lr=2e-3, seed=1, log=print):
     log(f"trained {steps} Adam steps in {t_train:.2f} s: loss {loss:.3e}; relative error of the projections "
         f"train {err_train:.4f}, test {err_test:.4f} (mean of the training set: {base:.4f})")
     np.savez(out, params=net.params, n_in=X.shape[1], width=width, n_out=W.shape[1], y_mean=mu, y_std=sd,
-             lam_scale=float(d["lam_scale"]), desc=d["desc"], shapes=d["shapes"], dim=int(d["dim"]),
+             lam_scale=float(d["lam_scale"]), desc=d["desc"], shapes=d["shapes"], rank=d["rank"], dim=int(d["dim"]),
              workload=str(d["workload"]), perturb_seed0=int(d["perturb_seed0"]), nperturb=int(d["nperturb"]),
              ntrain=ntrain, variant_seed=int(d["variant_seed"]), err_train=err_train, err_test=err_test)
     net.close()
@@ -126,14 +134,14 @@ class LearnedStart:
         self.mu, self.sd = np.asarray(m["y_mean"]), np.asarray(m["y_std"])
         self.net = Network(int(m["n_in"]), int(m["width"]), int(m["n_out"]), device=device)
         self.net.params = m["params"]
-        self.comp = Compressor(m["desc"], m["shapes"], int(m["dim"]))
+        self.comp = Compressor(m["desc"], m["shapes"], int(m["dim"]), m["rank"])
         self.dim = int(m["dim"])
 
     def projections(self, lam):
         x = np.asarray(lam, dtype=np.float32).reshape(1, -1) / self.lam_scale
         return self.net.forward(x)[0] * self.sd + self.mu
 
-    def start_vector(self, S, lam, beta=0.1, seed=5):
+    def start_vector(self, S, lam, beta=1.0, seed=5):
         """Start vector for the variant lam on solver S, or None (fallback: the standard start)
         when the model does not describe S's vector space."""
         if S.dim != self.dim:
@@ -149,7 +157,7 @@ class LearnedStart:
         self.net.close()
 
 
-def compare(S, fam, learned, lams, nev=10, tol=1e-4, beta=0.1, log=print):
+def compare(S, fam, learned, lams, nev=10, tol=1e-4, beta=1.0, log=print):
     """Standard vs learned start on the given variants: iterations, seconds, eigenvalues."""
     from ..nsx import NSX_FP32
     rows = []
@@ -178,15 +186,15 @@ def main():
     ap.add_argument("--K", type=int, default=256)
     ap.add_argument("--data", default="sweep.npz")
     ap.add_argument("--model", default="model.npz")
-    ap.add_argument("--train", type=int, default=400)
+    ap.add_argument("--train", type=int, default=400)   # training variants (the rest are held out)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--count", type=int, default=8)
-    ap.add_argument("--beta", type=float, default=0.1)
+    ap.add_argument("--beta", type=float, default=1.0)
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     if a.cmd == "sweep":
-        sweep(a.workload, a.variants, a.seed, a.K, a.out or a.data)
+        sweep(a.workload, a.variants, a.seed, a.K, a.out or a.data, ntrain=a.train)
     elif a.cmd == "train":
         print(json.dumps(train(a.data, a.train, a.out or a.model, steps=a.steps, lr=a.lr)))
     else:

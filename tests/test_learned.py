@@ -105,7 +105,7 @@ def test_learned_start_saves_iterations_on_held_out_variants(tmp_path):
     build()
     data = str(tmp_path / "sweep.npz")
     model = str(tmp_path / "model.npz")
-    L.sweep("fp_4p4n_0", 60, 11, 256, data, log=lambda *a: None)
+    L.sweep("fp_4p4n_0", 60, 11, 256, data, ntrain=48, log=lambda *a: None)
     stats = L.train(data, 48, model, width=256, steps=1500, lr=2e-3, log=lambda *a: None)
     assert stats["err_test"] < stats["err_mean_predictor"]   # the network beats predicting the mean
     learned = L.LearnedStart(model)
