@@ -214,8 +214,9 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
 
 // ---------------------------------------------------------------------------
 // k_z: one CTA per (group, P_r, 128-column tile); thread = column.  For each row
-// of P_r the group's sources are read once into registers and every operator's
-// mixed row is written to its Zbar slab.
+// of P_r the group's sources are read once into registers (NS of them at most: 16,
+// or ZMAXS when the plan has a larger group) and every operator's mixed row is
+// written to its Zbar slab.
 template <typename T, int NS>
 __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], const int64_t *ysrc, const int64_t *zdst,
                                         int ns, int na, const T *__restrict__ Y, T *__restrict__ Zb) {
@@ -231,12 +232,12 @@ __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], co
       T z = T(0);
 #pragma unroll
       for (int s = 0; s < NS; ++s) z = fma(ws[a][s], y[s], z);
-      Zb[zdst[a] + (int64_t)rr * u.d_bl + col] = z;
+      Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
     }
   }
 }
 
-template <typename T>
+template <typename T, int NS>
 __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, const ZGroup *__restrict__ groups,
                                            const ZSrc *__restrict__ srcs, const ZOp *__restrict__ ops,
                                            const T *__restrict__ W, const T *__restrict__ Y, T *__restrict__ Zb) {
@@ -253,99 +254,140 @@ __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, cons
   for (int e = threadIdx.x; e < na; e += blockDim.x) zdst[e] = ops[u.op_begin + e].z;
   for (int e = threadIdx.x; e < ZMAXS; e += blockDim.x) ysrc[e] = e < G.ns ? srcs[G.s_begin + e].y : 0;
   __syncthreads();
-  if (G.ns <= 16)
-    kz_body<T, 16>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
-  else
-    kz_body<T, 32>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
+  kz_body<T, NS>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
 }
 
 // ---------------------------------------------------------------------------
-// k_a: one CTA per (output slab P_l, 128-column tile, K range); 256 threads =
-// 4 row slots x 64 column pairs; slot s owns rows [s*RPT, s*RPT + RPT) with RPT
-// the smallest of 1, 2, 4, 8, 16 that covers nl.  Abar is staged in shared
-// memory in chunks of KC stacked rows; each thread streams its two Zbar
-// columns four rows at a time.  The K ranges of one tile add their partial
-// sums to the output with atomic adds (the like-particle stage wrote it first).
-constexpr int KA_KC = 128;
-template <typename T, int RPT>
-__device__ __forceinline__ void ka_body(const ATile &t, const T *__restrict__ Abar, const T *__restrict__ Zb,
-                                        T *__restrict__ out, T *as) {
-  const int nl = t.nl;
-  const int rs = threadIdx.x / 64, cp = threadIdx.x % 64;
-  const int c0 = 2 * cp, c1 = 2 * cp + 1;
-  const bool v0 = c0 < t.ncols, v1 = c1 < t.ncols;
-  const int lb = rs * RPT;
-  T acc0[RPT], acc1[RPT];
-#pragma unroll
-  for (int j = 0; j < RPT; ++j) acc0[j] = acc1[j] = T(0);
-  const T *Z = Zb + t.zbar;
-  for (int k0 = t.k_begin; k0 < t.k_end; k0 += KA_KC) {
-    const int kc = min(KA_KC, t.k_end - k0);
-    const T *Ak = Abar + t.abar + (int64_t)k0 * nl;
-    for (int e = threadIdx.x; e < kc * nl; e += blockDim.x) as[e] = Ak[e];
-    __syncthreads();
-    if (lb < nl) {
-      int k = 0;
-      for (; k + 4 <= kc; k += 4) {
-        T z0[4], z1[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const T *Zr = Z + (int64_t)(k0 + k + u) * t.ldz;
-          z0[u] = v0 ? Zr[c0] : T(0);
-          z1[u] = v1 ? Zr[c1] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const T *ak = as + (k + u) * nl + lb;
-#pragma unroll
-          for (int j = 0; j < RPT; ++j) {
-            const T a = (lb + j < nl) ? ak[j] : T(0);
-            acc0[j] = fma(a, z0[u], acc0[j]);
-            acc1[j] = fma(a, z1[u], acc1[j]);
-          }
-        }
-      }
-      for (; k < kc; ++k) {
-        const T *Zr = Z + (int64_t)(k0 + k) * t.ldz;
-        const T z0 = v0 ? Zr[c0] : T(0);
-        const T z1 = v1 ? Zr[c1] : T(0);
-        const T *ak = as + k * nl + lb;
-#pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-          const T a = (lb + j < nl) ? ak[j] : T(0);
-          acc0[j] = fma(a, z0, acc0[j]);
-          acc1[j] = fma(a, z1, acc1[j]);
-        }
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int j = 0; j < RPT; ++j) {
-    const int l = lb + j;
-    if (l < nl) {
-      if (v0) atomicAdd(out + t.out + l + (int64_t)t.ld * c0, acc0[j]);
-      if (v1) atomicAdd(out + t.out + l + (int64_t)t.ld * c1, acc1[j]);
-    }
-  }
+// k_a: one CTA of 128 threads per (output slab P_l, 128-column tile, K range).
+// The tile's Zbar rows (128 columns each, 16-byte aligned rows) and the matching
+// Abar rows (nlp entries each) stream through a 3-stage shared-memory pipeline of
+// asynchronous 16-byte copies, KS stacked rows per stage.  Within a stage the 4
+// warps split the rows; lane q owns columns 4q .. 4q+3 and accumulates a group of
+// RG output rows for them in registers (one 16-byte Zbar load and RG/4 broadcast
+// 16-byte Abar loads per stacked row, 4*RG FMAs).  Slabs with more than RG rows
+// take several passes.  At the end of a pass the warps' partial sums are added
+// through shared memory and the tile adds its result to the output with atomic
+// adds (K ranges of one slab are separate tiles; the like-particle stage wrote
+// the output first).
+template <typename T> struct KaCfg;
+template <> struct KaCfg<float> { static constexpr int KS = 16, RG = 16; };
+template <> struct KaCfg<double> { static constexpr int KS = 8, RG = 8; };
+constexpr int KA_STAGES = 3;
+constexpr int KA_MAXNL = 64;
+
+__device__ __forceinline__ void ka_cp16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void ka_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ka_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void ka_ld4(const float *p, float v[4]) {
+  const float4 q = *reinterpret_cast<const float4 *>(p);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ka_ld4(const double *p, double v[4]) {
+  const double2 a = *reinterpret_cast<const double2 *>(p);
+  const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
+struct KaSmem {
+  static constexpr int KS = KaCfg<T>::KS, RG = KaCfg<T>::RG;
+  static constexpr size_t pipe = sizeof(T) * (size_t)KA_STAGES * KS * (KA_TILE_COLS + KA_MAXNL);
+  static constexpr size_t red = sizeof(T) * (size_t)4 * RG * KA_TILE_COLS;
+  static constexpr size_t bytes = pipe > red ? pipe : red;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
                                            const T *__restrict__ Zb, T *__restrict__ out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *as = reinterpret_cast<T *>(smem_raw);  // [KC][nl]
+  constexpr int KS = KaCfg<T>::KS, RG = KaCfg<T>::RG, TC = KA_TILE_COLS;
+  constexpr int CPR = TC * (int)sizeof(T) / 16;                  // 16-byte chunks per Zbar row
+  __shared__ __align__(16) unsigned char raw[KaSmem<T>::bytes];
+  T *zs = reinterpret_cast<T *>(raw);                             // [KA_STAGES][KS][TC]
+  T *as = zs + (size_t)KA_STAGES * KS * TC;                       // [KA_STAGES][KS * nlp]
+  T *red = reinterpret_cast<T *>(raw);                            // [4][RG][TC] after a pass
   const ATile t = tiles[blockIdx.x];
-  if (t.nl <= 4)
-    ka_body<T, 1>(t, Abar, Zb, out, as);
-  else if (t.nl <= 8)
-    ka_body<T, 2>(t, Abar, Zb, out, as);
-  else if (t.nl <= 16)
-    ka_body<T, 4>(t, Abar, Zb, out, as);
-  else if (t.nl <= 32)
-    ka_body<T, 8>(t, Abar, Zb, out, as);
-  else
-    ka_body<T, 16>(t, Abar, Zb, out, as);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nl = t.nl, nlp = t.nlp;
+  const int ncp = (t.ncols * (int)sizeof(T) + 15) / 16;         // chunks per row that hold tile columns
+  const int nchunk = (t.k_end - t.k_begin + KS - 1) / KS;
+  const T *Zt = Zb + t.zbar;
+  const T *At = Abar + t.abar;
+
+  auto load = [&](int c, int b) {
+    const int k0 = t.k_begin + c * KS;
+    const int kc = min(KS, t.k_end - k0);
+    T *zb = zs + (size_t)b * KS * TC;
+    for (int e = tid; e < kc * CPR; e += 128) {
+      const int r = e / CPR, q = e - r * CPR;
+      if (q < ncp) ka_cp16(zb + r * TC + q * (16 / (int)sizeof(T)), Zt + (int64_t)(k0 + r) * t.ldz + q * (16 / (int)sizeof(T)));
+    }
+    T *ab = as + (size_t)b * KS * KA_MAXNL;
+    const int na = kc * nlp * (int)sizeof(T) / 16;
+    const T *asrc = At + (int64_t)k0 * nlp;
+    for (int e = tid; e < na; e += 128) ka_cp16(ab + e * (16 / (int)sizeof(T)), asrc + e * (16 / (int)sizeof(T)));
+  };
+
+  for (int l0 = 0; l0 < nl; l0 += RG) {
+    T acc[RG][4];
+#pragma unroll
+    for (int i = 0; i < RG; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[i][c] = T(0);
+    const int ng = min(RG, nlp - l0) / 4;                        // groups of 4 rows with Abar entries
+#pragma unroll
+    for (int s = 0; s < KA_STAGES - 1; ++s) {
+      if (s < nchunk) load(s, s);
+      ka_commit();
+    }
+    for (int c = 0; c < nchunk; ++c) {
+      if (c + KA_STAGES - 1 < nchunk) load(c + KA_STAGES - 1, (c + KA_STAGES - 1) % KA_STAGES);
+      ka_commit();
+      ka_wait<KA_STAGES - 1>();
+      __syncthreads();
+      const int b = c % KA_STAGES;
+      const int kc = min(KS, t.k_end - (t.k_begin + c * KS));
+      const T *zb = zs + (size_t)b * KS * TC + 4 * lane;
+      const T *ab = as + (size_t)b * KS * KA_MAXNL + l0;
+      for (int r = warp; r < kc; r += 4) {
+        T z[4];
+        ka_ld4(zb + r * TC, z);
+        const T *ar = ab + r * nlp;
+#pragma unroll
+        for (int g = 0; g < RG / 4; ++g) {
+          if (g < ng) {
+            T a[4];
+            ka_ld4(ar + 4 * g, a);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int cc = 0; cc < 4; ++cc) acc[4 * g + i][cc] = fma(a[i], z[cc], acc[4 * g + i][cc]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    ka_wait<0>();
+    // add the 4 warps' partial sums and the result to the output
+#pragma unroll
+    for (int i = 0; i < RG; ++i)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) red[((size_t)warp * RG + i) * TC + 4 * lane + cc] = acc[i][cc];
+    __syncthreads();
+    if (tid < t.ncols) {
+      for (int i = 0; i < RG && l0 + i < nl; ++i) {
+        T v = red[(size_t)i * TC + tid];
+#pragma unroll
+        for (int w = 1; w < 4; ++w) v += red[((size_t)w * RG + i) * TC + tid];
+        atomicAdd(out + t.out + (l0 + i) + (int64_t)t.ld * tid, v);
+      }
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void k_d2f(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
@@ -378,7 +420,6 @@ static S *dev_copy_pod(const std::vector<S> &v) {
   return p;
 }
 
-static size_t ka_smem(const nsx_handle *h, size_t es) { return es * (size_t)KA_KC * std::max(h->max_anl, 1); }
 
 template <typename T>
 static void dev_refill(T *p, const std::vector<double> &v) {
@@ -406,7 +447,7 @@ void upload_interaction(nsx_handle *h) {
 
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
-  if (h->max_anl > 64) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
+  if (h->max_anl > KA_MAXNL) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
   d.rhoA = dev_copy<double>(h->A.vals);
   d.rhoB = dev_copy<double>(h->yrho);
@@ -427,10 +468,8 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
   for (size_t es : {sizeof(double), sizeof(float)}) {
-    if (ka_smem(h, es) > 227 * 1024) fail(NSX_E_ARG, "density sub-blocks too large for the shared-memory staging of k_a");
+    (void)es;
   }
-  NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 8)));
-  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ka_smem(h, 4)));
 }
 
 void ensure_precision(nsx_handle *h, int precision) {
@@ -529,11 +568,15 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->zunits.empty()) {
     StageScope sc(h, 2, s);
-    k_z<T><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
+    // sources per group: registers for 16 unless the plan has a larger group
+    if (h->max_zns <= 16)
+      k_z<T, 16><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
+    else
+      k_z<T, ZMAXS><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
   }
   if (!h->atiles.empty()) {
     StageScope sc(h, 3, s);
-    k_a<T><<<(unsigned)h->atiles.size(), 256, ka_smem(h, sizeof(T)), s>>>(d.atiles, abar, Z, out);
+    k_a<T><<<(unsigned)h->atiles.size(), 128, 0, s>>>(d.atiles, abar, Z, out);
   }
   NSX_CUDA(cudaGetLastError());
 }
@@ -561,13 +604,13 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   }
 }
 
-// The FP64 stages with a caller-provided scratch buffer: Y (y_elems, zero where no
-// density block reaches) followed by Zbar (z_elems).  Used by the fixed-scratch entry point.
+// The FP64 stages with a caller-provided scratch buffer: Y (y_elems) and Zbar (z_elems) from
+// zbar_scratch_offset(h).  Used by the fixed-scratch entry point.
 void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s) {
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = NSX_FP64;
-  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + h->y_elems, s);
+  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
 }
 
 void release(nsx_handle *h) {

@@ -16,10 +16,10 @@
 //   that first call before any stream capture.  Every GPU that loads the
 //   library holds the array until the process exits.
 // * All calls share the one array and it keeps the last call's contents; the
-//   part the product needs zeroed (the Y slabs no density block reaches) is
-//   cleared at the start of every call on the caller's stream.  Calls that
-//   overlap on the GPU (different streams, or different handles on the same
-//   device, without ordering) race on the array.
+//   product writes every scratch element it later reads, so the previous
+//   call's contents do not matter and nothing is cleared.  Calls that overlap
+//   on the GPU (different streams, or different handles on the same device,
+//   without ordering) race on the array.
 #include <mutex>
 #include "nsx_internal.h"
 
@@ -53,7 +53,7 @@ int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream) {
   if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
   if (x == y) fail(NSX_E_ARG, "x and y must not alias");
-  const int64_t need = h->y_elems + h->z_elems;
+  const int64_t need = zbar_scratch_offset(h) + h->z_elems;
   if (need > NOALLOC_Y_MAX)
     fail(NSX_E_ARG, "problem needs " + std::to_string(need) + " FP64 scratch elements; the fixed array of "
                         "nsx_matvec_noalloc holds " + std::to_string(NOALLOC_Y_MAX) + " (use nsx_matvec)");

@@ -105,25 +105,33 @@ struct ZUnit {              // (group, P_r, column tile)
   int32_t grp;
   int32_t row0, nr;         // rows of P_r in the J_ar space
   int32_t c0, ncols;        // column tile
-  int32_t d_bl;             // row length of Y and Zbar
+  int32_t d_bl;             // row length of Y
   int32_t op_begin, op_end; // range in zops
+  int32_t ldz;              // row length of Zbar (d_bl rounded up to KZ_PAD)
+  int32_t pad;
 };
+// Zbar rows are padded to a multiple of KZ_PAD elements and every slab starts at a multiple of
+// KZ_PAD, so that each row of a 128-column tile starts on a 16-byte boundary (asynchronous
+// 16-byte copies into shared memory in k_a, FP32 and FP64); Abar rows likewise (nl -> nlp).
+constexpr int KZ_PAD = 4;
 struct ZOp {
-  int64_t z;                // Zbar destination of the operator: element (row rr of P_r, col c) at z + rr*d_bl + c
+  int64_t z;                // Zbar destination of the operator: element (row rr of P_r, col c) at z + rr*ldz + c
   int32_t wrow;             // weight row within the group
   int32_t pad;
 };
-// Proton side k_a: out[P_l rows, cols] += Abar (nl x K, column-major) * Zbar (K x d_bl, row-major).
+// Proton side k_a: out[P_l rows, cols] += Abar (nl x K, column-major, leading dimension nlp) *
+// Zbar (K x d_bl, row-major, leading dimension ldz).
 constexpr int KA_TILE_COLS = 128;   // output columns per k_a tile (64 threads x 2 columns)
 struct ATile {
   int64_t out;      // element offset of out[P_l row 0, col0]
   int32_t ld;       // d_al (leading dimension of the output block)
   int32_t nl;       // rows = nJT(P_l, J_al)
   int32_t col0, ncols;
-  int32_t ldz;      // d_bl
+  int32_t ldz;      // Zbar row length (d_bl rounded up to KZ_PAD)
   int32_t k_begin, k_end;  // range of stacked contribution rows handled by this tile
+  int32_t nlp;      // Abar leading dimension (nl rounded up to KZ_PAD; padding rows are zero)
   int64_t zbar;     // offset of Zbar[0, col0]
-  int64_t abar;     // offset of Abar[0, 0]
+  int64_t abar;     // offset of Abar[0, 0] of the slab
 };
 // like-particle part: out_blk = Ha C + C Hb, 64x64 output tiles.
 struct LTile {
@@ -182,7 +190,7 @@ struct nsx_handle {
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
   int64_t y_elems = 0, z_elems = 0;
-  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_ldy = 0;
+  int max_ynl = 0, max_ynr = 0, max_anl = 0, max_ldy = 0, max_zns = 0;
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -196,6 +204,10 @@ struct nsx_handle {
 };
 
 namespace nsx {
+// Offset of Zbar in a caller-provided FP64 scratch buffer that holds Y then Zbar: Y's length
+// rounded up to 32 elements, so that Zbar starts on a 256-byte boundary (k_a copies its rows
+// with 16-byte asynchronous copies).
+inline int64_t zbar_scratch_offset(const nsx_handle *h) { return (h->y_elems + 31) / 32 * 32; }
 void build_plan(nsx_handle *h, const nsx_problem *p);
 void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
                      const double *b_seg_vals, int64_t b_nvals);

@@ -451,11 +451,12 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     }
   }
   // Zbar slabs and Abar
+  auto padz = [](int64_t n) { return (n + KZ_PAD - 1) / KZ_PAD * KZ_PAD; };
   std::vector<int64_t> zoff(slabs.size());
   int64_t ztot = 0;
   for (size_t sl = 0; sl < slabs.size(); ++sl) {
     zoff[sl] = ztot;
-    ztot += (int64_t)slabK[sl] * h->blocks[slabs[sl].first].db;
+    ztot += (int64_t)slabK[sl] * padz(h->blocks[slabs[sl].first].db);
   }
   // k_z units: (group, P_r, 128-column tile)
   const int ZT = 128;
@@ -463,7 +464,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     const int bl = slabs[pd.ops[0].slab].first;
     const Block &ob = h->blocks[bl];
     int op0 = (int)h->zops.size();
-    for (const PendingOp &o : pd.ops) h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ob.db, o.wrow, 0});
+    const int ldz = (int)padz(ob.db);
+    for (const PendingOp &o : pd.ops) h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ldz, o.wrow, 0});
     int op1 = (int)h->zops.size();
     for (int c0 = 0; c0 < ob.db; c0 += ZT) {
       ZUnit u;
@@ -475,6 +477,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       u.d_bl = ob.db;
       u.op_begin = op0;
       u.op_end = op1;
+      u.ldz = ldz;
+      u.pad = 0;
       h->zunits.push_back(u);
     }
   }
@@ -483,10 +487,14 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   for (size_t sl = 0; sl < slabs.size(); ++sl) {
     const int bl = slabs[sl].first, pl = slabs[sl].second;
     const Block &ob = h->blocks[bl];
-    int64_t a0 = (int64_t)h->abar.size();
-    for (auto &bv : slab_blocks[sl]) {
-      int nl = A.njt_of(pl, ob.J2a);
-      h->abar.insert(h->abar.end(), A.vals.begin() + bv.second, A.vals.begin() + bv.second + (int64_t)nl * bv.first);
+    const int nl = A.njt_of(pl, ob.J2a), nlp = (int)padz(nl);
+    h->abar.resize(padz((int64_t)h->abar.size()), 0.0);
+    const int64_t a0 = (int64_t)h->abar.size();
+    for (auto &bv : slab_blocks[sl]) {   // bv = (nr, offset of the nl x nr density block)
+      const int64_t at = (int64_t)h->abar.size();
+      h->abar.resize(at + (int64_t)nlp * bv.first, 0.0);
+      for (int k = 0; k < bv.first; ++k)
+        for (int l = 0; l < nl; ++l) h->abar[at + (int64_t)nlp * k + l] = A.vals[bv.second + (int64_t)nl * k + l];
     }
     for (int c0 = 0; c0 < ob.db; c0 += TW)
       for (int kb = 0; kb < slabK[sl]; kb += KA_K_SPLIT) {
@@ -496,9 +504,10 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
         t.nl = A.njt_of(pl, ob.J2a);
         t.col0 = c0;
         t.ncols = std::min(TW, ob.db - c0);
-        t.ldz = ob.db;
+        t.ldz = (int)padz(ob.db);
         t.k_begin = kb;
         t.k_end = std::min(slabK[sl], kb + KA_K_SPLIT);
+        t.nlp = nlp;
         t.zbar = zoff[sl] + c0;
         t.abar = a0;
         h->atiles.push_back(t);
@@ -517,6 +526,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     h->max_ynr = std::max(h->max_ynr, y.nr);
   }
   for (auto &t : h->atiles) h->max_anl = std::max(h->max_anl, t.nl);
+  h->max_zns = 0;
+  for (auto &g : h->zgroups) h->max_zns = std::max(h->max_zns, g.ns);
 }
 
 }  // namespace nsx
