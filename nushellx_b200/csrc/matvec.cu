@@ -19,6 +19,7 @@
 // Each intermediate (Y, Zbar) is written once and read once, in row streams.
 // Templated on the contraction type: double (the FP64 form) or float (the FP32
 // form, FP64 vectors converted at the boundary).
+#include <type_traits>
 #include <algorithm>
 #include <cstdio>
 #include "nsx_internal.h"
@@ -86,7 +87,8 @@ __global__ void __launch_bounds__(256) k_like(const LTile *__restrict__ tiles, c
 }
 
 // ---------------------------------------------------------------------------
-// k_y: one CTA per (Y matrix, 256-row tile); thread = rows t and t + 128.
+// k_y: one CTA per (Y matrix, 256-row tile); FP64: thread = rows t and t + 128;
+// FP32: warp w = rows 64w .. 64w + 63 on the tensor cores (ky_piece_tc below).
 // The tile's part of Y (256 consecutive rows of a row-major matrix) is produced
 // in column windows of at most 128 bytes (32 FP32 / 16 FP64 columns).  A window
 // holds whole neutron density sub-blocks (Q_l, Q_r); a sub-block wider than the
@@ -157,6 +159,113 @@ __device__ __forceinline__ void ky_piece(const T *__restrict__ c0, bool ok0, boo
   }
 }
 
+// FP32 pieces on the tensor cores: mma.sync m16n8k8 TF32 with the 3xTF32 split
+// (x = big + small, both TF32; big*big + big*small + small*big accumulated in FP32),
+// which keeps FP32 accuracy.  Fragment layouts (PTX ISA, m16n8k8 .tf32), with
+// g = lane / 4 and q = lane % 4:  A (16 x 8, row-major) a0 = (g, q), a1 = (g+8, q),
+// a2 = (g, q+4), a3 = (g+8, q+4);  B (8 x 8, column-major) b0 = (k q, n g),
+// b1 = (k q+4, n g);  D (16 x 8) d0 = (g, 2q), d1 = (g, 2q+1), d2 = (g+8, 2q),
+// d3 = (g+8, 2q+1).
+__device__ __forceinline__ uint32_t ky_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void ky_split(float x, uint32_t &big, uint32_t &small) {
+  big = ky_tf32(x);
+  small = ky_tf32(x - __uint_as_float(big));
+}
+__device__ __forceinline__ void ky_mma(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Rows [wr0, wr0 + 32) of the tile (two m16 tiles) for outputs l in [plo, phi)
+// (plo a multiple of 8, NT = ceil((phi - plo) / 8) n8 tiles) of one sub-block:
+// C points at C_h[row0 of the tile, Q_r col 0]; tcol at the tile column of output 0.
+template <int NT>
+__device__ __forceinline__ void ky_piece_tc(const float *__restrict__ C, int64_t m, int rows, int wr0, int nr,
+                                            const float *__restrict__ rb, int ldr, int plo, int phi, float *tcol,
+                                            int ld) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  float acc[2][NT][4];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.f;
+  const float *cr[2][2];
+  bool rok[2][2];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = wr0 + 16 * mt + g + 8 * h;
+      rok[mt][h] = r < rows;
+      cr[mt][h] = C + r;
+    }
+  for (int k0 = 0; k0 < nr; k0 += 8) {
+    const int ka = k0 + q, kb = k0 + q + 4;
+    const bool kaok = ka < nr, kbok = kb < nr;
+    uint32_t abig[2][4], asml[2][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const float v0 = (rok[mt][0] && kaok) ? cr[mt][0][m * ka] : 0.f;
+      const float v1 = (rok[mt][1] && kaok) ? cr[mt][1][m * ka] : 0.f;
+      const float v2 = (rok[mt][0] && kbok) ? cr[mt][0][m * kb] : 0.f;
+      const float v3 = (rok[mt][1] && kbok) ? cr[mt][1][m * kb] : 0.f;
+      ky_split(v0, abig[mt][0], asml[mt][0]);
+      ky_split(v1, abig[mt][1], asml[mt][1]);
+      ky_split(v2, abig[mt][2], asml[mt][2]);
+      ky_split(v3, abig[mt][3], asml[mt][3]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int l = plo + 8 * nt + g;
+      const float w0 = kaok ? __ldg(rb + l + (int64_t)ldr * ka) : 0.f;
+      const float w1 = kbok ? __ldg(rb + l + (int64_t)ldr * kb) : 0.f;
+      uint32_t b0, b0s, b1, b1s;
+      ky_split(w0, b0, b0s);
+      ky_split(w1, b1, b1s);
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        ky_mma(acc[mt][nt], asml[mt], b0, b1);
+        ky_mma(acc[mt][nt], abig[mt], b0s, b1s);
+        ky_mma(acc[mt][nt], abig[mt], b0, b1);
+      }
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int l = plo + 8 * nt + 2 * q;
+      float *t0 = tcol + (wr0 + 16 * mt + g) * ld;
+      float *t1 = t0 + 8 * ld;
+      if (l < phi) {
+        t0[l] = acc[mt][nt][0];
+        t1[l] = acc[mt][nt][2];
+      }
+      if (l + 1 < phi) {
+        t0[l + 1] = acc[mt][nt][1];
+        t1[l + 1] = acc[mt][nt][3];
+      }
+    }
+}
+
+__device__ __forceinline__ void ky_piece_tc_any(const float *C, int64_t m, int rows, int wr0, int nr,
+                                                const float *rb, int ldr, int plo, int phi, float *tcol, int ld) {
+  switch ((phi - plo + 7) >> 3) {
+    case 1: ky_piece_tc<1>(C, m, rows, wr0, nr, rb, ldr, plo, phi, tcol, ld); break;
+    case 2: ky_piece_tc<2>(C, m, rows, wr0, nr, rb, ldr, plo, phi, tcol, ld); break;
+    case 3: ky_piece_tc<3>(C, m, rows, wr0, nr, rb, ldr, plo, phi, tcol, ld); break;
+    default: ky_piece_tc<4>(C, m, rows, wr0, nr, rb, ldr, plo, phi, tcol, ld); break;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
                                            const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
@@ -191,10 +300,20 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
         nbi = j;
         nlst = hi;
       }
-      T *t = tile + tid * LD + (b.ycol - ws);
-      const T *c0 = C + m * b.ccol;
-      if (mode == 2) ky_piece<T, 2>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
-      else if (mode == 1) ky_piece<T, 1>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
+      if constexpr (std::is_same<T, float>::value) {
+        // tensor cores: warp w owns tile rows [64w, 64w + 64) in two halves of 32
+        const float *Cb = x + g.c_base + g.row0 + m * b.ccol;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          const int wr0 = 64 * (tid >> 5) + 32 * half;
+          if (wr0 < rows) ky_piece_tc_any(Cb, m, rows, wr0, b.nr, rho + b.rho, b.ldr, l0, hi, tile + (b.ycol - ws), LD);
+        }
+      } else {
+        T *t = tile + tid * LD + (b.ycol - ws);
+        const T *c0 = C + m * b.ccol;
+        if (mode == 2) ky_piece<T, 2>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
+        else if (mode == 1) ky_piece<T, 1>(c0, ok0, ok1, m, rho + b.rho, b.ldr, b.nr, l0, hi, t, 128 * LD);
+      }
       if (hi < b.nl) break;
     }
     __syncthreads();
