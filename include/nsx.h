@@ -171,6 +171,20 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs,
               nsx_report *report);
 
+/* Write eigenpairs (evals[nev], evecs[nev][no_state], e.g. from nsx_solve) in the
+ * reference's output files, as NuTRL leaves them for NuVec (src/NuLnz/NuCoreX.f90:526-533,
+ * 280-281; src/NuVec/NuVec.f90:120-131, 285-286, 298-321):
+ *   <prefix>.abz  thick-restart form, 4 records: isave = nev, alpha = E, betat = 0,
+ *                 matrix = diag(E); imax = iterations, no_level = nev, tt, no_state, basd,
+ *                 count = 2, no_keep = no_conv = nev, first_iter, second_iter, noiter;
+ *                 bas; alpha_copy, betat(isave+1), indx
+ *   <prefix>.trl  one FP32 direct-access record of no_state values per eigenvector
+ *   <prefix>.lev  header (intfile, 2J and 2T = T2) and the levels as 5(f10.3,a1)
+ * NuVec's reconstruction from these files returns exactly the given eigenpairs.
+ * The reference names prefix Nucleus // file_code(J2/2, no_cA, no_cB). */
+int nsx_write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs,
+                      int32_t nev, int32_t iterations, const char *intfile, int32_t T2);
+
 /* Device-side statistics of a handle (for benchmarking and profiling).
  * Stages of one H.v: 0 = like-particle products (k_like), 1 = neutron-side Y
  * products (k_y), 2 = mixing into the stacked operands (k_z), 3 = proton-side

@@ -140,6 +140,13 @@ module nsx_iface
        type(c_ptr), value :: evecs                     ! c_loc(vectors(1,1)) or c_null_ptr
        type(nsx_report), intent(out) :: report
      end function
+     integer(c_int) function nsx_write_results(h, prefix, evals, evecs, nev, iterations, intfile, T2) &
+          bind(C, name="nsx_write_results")
+       import :: c_int, c_int32_t, c_double, c_ptr
+       type(c_ptr), value :: h, prefix, intfile           ! prefix, intfile: c_loc of NUL-terminated strings
+       real(c_double), intent(in) :: evals(*), evecs(*)
+       integer(c_int32_t), value :: nev, iterations, T2
+     end function
      integer(c_int) function nsx_stats_reset(h, timing) bind(C, name="nsx_stats_reset")
        import :: c_int, c_int32_t, c_ptr
        type(c_ptr), value :: h

@@ -37,6 +37,8 @@ def build(verbose=False, force=False):
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
     headers.append(os.path.join(INCLUDE, "nsx.h"))
     if not force and not _stale(LIB, srcs + headers):
+        if _stale(CLI, [CLI_SRC, LIB]):
+            build_cli(verbose)
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -55,7 +57,22 @@ def build(verbose=False, force=False):
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    build_cli(verbose)
     return LIB
+
+
+CLI_SRC = os.path.join(HERE, "cli", "nulnz_gpu.cpp")
+CLI = os.path.join(HERE, "nulnz_gpu")
+
+
+def build_cli(verbose=False):
+    """The nulnz_gpu command (C++ host over the C ABI), linked against libnsx.so."""
+    cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, CLI_SRC, "-o", CLI, "-L", HERE, "-lnsx",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return CLI
 
 
 if __name__ == "__main__":

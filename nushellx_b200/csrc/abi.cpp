@@ -94,6 +94,14 @@ int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const
   });
 }
 
+int nsx_write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs,
+                      int32_t nev, int32_t iterations, const char *intfile, int32_t T2) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    write_results(h, prefix, evals, evecs, nev, iterations, intfile, T2);
+  });
+}
+
 int64_t nsx_dim(const nsx_handle *h) { return h ? h->no_state : 0; }
 int32_t nsx_nblocks(const nsx_handle *h) { return h ? (int32_t)h->blocks.size() : 0; }
 

@@ -219,6 +219,8 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
 void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s);
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]);
 void flush_stage_events(nsx_handle *h);
+void write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs, int nev,
+                   int iterations, const char *intfile, int T2);
 double sixj(int a, int b, int c, int d, int e, int f);
 double racah_w(int j1, int j2, int j3, int j4, int J, int K);
 }  // namespace nsx

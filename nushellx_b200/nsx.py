@@ -88,6 +88,8 @@ SYMBOLS = {
     "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
     "nsx_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
+    "nsx_write_results": (C.c_int, [C.c_void_p, C.c_char_p, _p(C.c_double), _p(C.c_double), C.c_int32, C.c_int32,
+                                    C.c_char_p, C.c_int32]),
     "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
     "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
     "nsx_destroy": (None, [C.c_void_p]),
@@ -300,6 +302,15 @@ class Solver:
         out = rep.as_dict()
         out["residual"] = [rep.residual[i] for i in range(min(nev, 64))]
         return ev, vecs, out
+
+    def write_results(self, prefix, evals, vecs, iterations=0, intfile="", T2=0):
+        """The reference's .abz / .trl / .lev files for these eigenpairs (nsx_write_results)."""
+        ev = np.ascontiguousarray(evals, dtype=np.float64)
+        vv = np.ascontiguousarray(vecs, dtype=np.float64)
+        assert vv.shape == (len(ev), self.dim)
+        _check(self._lib.nsx_write_results(self._h, prefix.encode(), ev.ctypes.data_as(_p(C.c_double)),
+                                           vv.ctypes.data_as(_p(C.c_double)), len(ev), int(iterations),
+                                           intfile.encode(), int(T2)))
 
     def stats_reset(self, timing=False):
         _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))
