@@ -171,6 +171,16 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs,
               nsx_report *report);
 
+/* Many independent solves at once (different J^pi, interaction variants or problems
+ * of uneven size): problem i is nsx_solve(handles[i], &params[i], evals[i],
+ * evecs ? evecs[i] : NULL, reports ? &reports[i] : NULL).  Every handle solves on its
+ * own non-blocking stream from a pool of host threads, so the small problems' kernels
+ * and host round trips overlap on the GPU.  The handles must be distinct.  Returns the
+ * first failing problem's code, with "problem i: ..." in nsx_last_error().  The
+ * reference runs one NuLnz process per J^pi (src/NuShellx/NuShellx.f90:1060-1061). */
+int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *params, double *const *evals,
+                    double *const *evecs, nsx_report *reports);
+
 /* Write eigenpairs (evals[nev], evecs[nev][no_state], e.g. from nsx_solve) in the
  * reference's output files, as NuTRL leaves them for NuVec (src/NuLnz/NuCoreX.f90:526-533,
  * 280-281; src/NuVec/NuVec.f90:120-131, 285-286, 298-321):

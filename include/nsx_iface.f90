@@ -140,6 +140,16 @@ module nsx_iface
        type(c_ptr), value :: evecs                     ! c_loc(vectors(1,1)) or c_null_ptr
        type(nsx_report), intent(out) :: report
      end function
+     integer(c_int) function nsx_batch_solve(handles, n, params, evals, evecs, reports) &
+          bind(C, name="nsx_batch_solve")
+       import :: c_int, c_int32_t, c_ptr, nsx_params, nsx_report
+       type(c_ptr), intent(in) :: handles(*)            ! one handle per problem
+       integer(c_int32_t), value :: n
+       type(nsx_params), intent(in) :: params(*)
+       type(c_ptr), intent(in) :: evals(*)              ! c_loc of each problem's eigenvalue array
+       type(c_ptr), value :: evecs                      ! c_loc of an array of n c_ptr, or c_null_ptr
+       type(nsx_report), intent(out) :: reports(*)
+     end function
      integer(c_int) function nsx_write_results(h, prefix, evals, evecs, nev, iterations, intfile, T2) &
           bind(C, name="nsx_write_results")
        import :: c_int, c_int32_t, c_double, c_ptr

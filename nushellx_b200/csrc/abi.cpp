@@ -1,8 +1,11 @@
 // extern "C" entry points of libnsx (declared in include/nsx.h).  Every call
 // catches internal failures and turns them into a negative return code plus a
 // thread-local message: nothing is thrown or aborted across the boundary.
+#include <atomic>
 #include <cstring>
 #include <memory>
+#include <thread>
+#include <vector>
 #include <exception>
 #include <new>
 #include "nsx_internal.h"
@@ -92,6 +95,45 @@ int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const
     set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals);
     upload_interaction(h);
   });
+}
+
+int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *params, double *const *evals,
+                    double *const *evecs, nsx_report *reports) {
+  int rc = guarded([&] {
+    if (!handles || !params || !evals) fail(NSX_E_ARG, "null argument");
+    if (n < 0 || n > 4096) fail(NSX_E_ARG, "problem count out of range (0 .. 4096)");
+    std::vector<nsx_handle *> hs(handles, handles + n);
+    for (int i = 0; i < n; ++i) {
+      if (!hs[i] || !evals[i]) fail(NSX_E_ARG, "null handle or eigenvalue array for problem " + std::to_string(i));
+      for (int j = 0; j < i; ++j)
+        if (hs[j] == hs[i]) fail(NSX_E_ARG, "the same handle is listed twice (problems " + std::to_string(j) +
+                                                " and " + std::to_string(i) + ")");
+    }
+  });
+  if (rc != NSX_OK || n == 0) return rc;
+  // one host worker per handle at a time, each solving on its handle's own stream
+  std::vector<int> codes(n, NSX_OK);
+  std::vector<std::string> msgs(n);
+  std::atomic<int> next{0};
+  const int workers = std::min<int>(n, 32);
+  std::vector<std::thread> pool;
+  for (int w = 0; w < workers; ++w)
+    pool.emplace_back([&] {
+      for (int i = next++; i < n; i = next++) {
+        codes[i] = guarded([&] {
+          NSX_CUDA(cudaSetDevice(handles[i]->device));
+          solve(handles[i], &params[i], evals[i], evecs ? evecs[i] : nullptr, reports ? &reports[i] : nullptr);
+        });
+        if (codes[i] != NSX_OK) msgs[i] = g_err;
+      }
+    });
+  for (auto &t : pool) t.join();
+  for (int i = 0; i < n; ++i)
+    if (codes[i] != NSX_OK) {
+      g_err = "problem " + std::to_string(i) + ": " + msgs[i];
+      return codes[i];
+    }
+  return NSX_OK;
 }
 
 int nsx_write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs,

@@ -18,6 +18,8 @@
 //   orthogonalised against the basis, with a zero coupling, as the reference
 //   does at NuCoreX.f90:368-382.
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -273,12 +275,31 @@ static void subtract(const double *V, int64_t ld, int cnt, const double *h, doub
   }
 }
 
+// Largest window (k_jacobi keeps two m x m FP64 matrices in shared memory) and the
+// shared-memory caps it implies.  The caps are kernel attributes shared by every host
+// thread, so they are set once per device to these maxima (never per launch: a
+// concurrent solve could otherwise lower the cap between another solve's setting and
+// its launch).
+constexpr int MAX_WINDOW = 112;
+constexpr size_t JACOBI_SMEM_MAX = sizeof(double) * (2 * (size_t)MAX_WINDOW * MAX_WINDOW + MAX_WINDOW) +
+                                   sizeof(int) * MAX_WINDOW;
+constexpr size_t ROTATE_SMEM_MAX = sizeof(double) * (size_t)MAX_WINDOW * MAX_WINDOW;
+
+static void ensure_kernel_attributes(int device) {
+  static std::mutex mu;
+  static std::set<int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(device)) return;
+  NSX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JACOBI_SMEM_MAX));
+  NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROTATE_SMEM_MAX));
+  done.insert(device);
+}
+
 static void jacobi(Workspace &ws, int m, const std::vector<double> &T, std::vector<double> &evals,
                    std::vector<double> &evecs, cudaStream_t s) {
   NSX_CUDA(cudaMemcpyAsync(ws.T, T.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, s));
   int mp = m + (m & 1);
   size_t smem = sizeof(double) * (2 * (size_t)mp * mp + mp) + sizeof(int) * mp;
-  NSX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   count_launch();
   k_jacobi<<<1, 512, smem, s>>>(ws.T, m, ws.ev, ws.S, ws.status);
   NSX_CUDA(cudaGetLastError());
@@ -350,7 +371,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   const int nev = (int)std::min<int64_t>(P->nev, nallowed);
   int m = P->window > 0 ? P->window : 100;
   m = (int)std::min<int64_t>(m, nallowed);
-  m = std::min(m, 112);  // k_jacobi keeps two m x m FP64 matrices in shared memory
+  m = std::min(m, MAX_WINDOW);
   if (m < nev + 1 && m < nallowed) fail(NSX_E_ARG, "window must exceed nev");
   int keep = P->keep > 0 ? P->keep : std::max(nev + 10, m / 3);
   keep = std::min(keep, m - 2);
@@ -358,8 +379,9 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   const int max_iter = P->max_iter > 0 ? P->max_iter : 2000;
   const double tol = P->tol > 0 ? P->tol : 1e-6;
   const int prec = P->precision;
-  cudaStream_t s = 0;
   ensure_precision(h, prec);
+  ensure_kernel_attributes(h->device);
+  cudaStream_t s = solve_stream(h);  // the handle's own non-blocking stream: solves of different handles overlap
   struct CounterScope {
     CounterScope(int64_t *p) { g_launches = p; }
     ~CounterScope() { g_launches = nullptr; }
@@ -378,14 +400,14 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   NSX_CUDA(cudaMalloc(&ws.S, sizeof(double) * m * m));
   NSX_CUDA(cudaMalloc(&ws.status, sizeof(int)));
   NSX_CUDA(cudaMalloc(&ws.mask, n));
-  NSX_CUDA(cudaMemcpy(ws.mask, h->lcoef.data(), n, cudaMemcpyHostToDevice));
+  NSX_CUDA(cudaMemcpyAsync(ws.mask, h->lcoef.data(), n, cudaMemcpyHostToDevice, s));
   Timer tm{h};
   int matvecs = 0, iters = 0, restarts = 0;
   auto V = [&](int j) { return ws.V + (int64_t)j * n; };
 
   // start vector
   if (P->start) {
-    NSX_CUDA(cudaMemcpy(V(0), P->start, sizeof(double) * n, cudaMemcpyHostToDevice));
+    NSX_CUDA(cudaMemcpyAsync(V(0), P->start, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   } else {
     count_launch();
     k_rand<<<grid_for(n), 256, 0, s>>>(V(0), ws.mask, n, P->seed ? P->seed : 5);
@@ -475,8 +497,6 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
         for (int r = 0; r < mm; ++r) Sk[r + (size_t)mm * c] = Sm[r + (size_t)mm * c];
       NSX_CUDA(cudaMemcpyAsync(ws.S, Sk.data(), sizeof(double) * Sk.size(), cudaMemcpyHostToDevice, s));
       size_t smem = sizeof(double) * mm * nev;
-      NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)std::max<size_t>(smem, 1024)));
       count_launch();
       k_rotate<<<grid_for(n), 256, smem, s>>>(ws.V, n, mm, ws.S, nev, ws.tmp, n);
       NSX_CUDA(cudaGetLastError());
@@ -493,8 +513,6 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
       for (int r = 0; r < m; ++r) Sk[r + (size_t)m * c] = Sm[r + (size_t)m * c];
     NSX_CUDA(cudaMemcpyAsync(ws.S, Sk.data(), sizeof(double) * Sk.size(), cudaMemcpyHostToDevice, s));
     size_t smem = sizeof(double) * m * keep;
-    NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<size_t>(smem, 1024)));
     count_launch();
     k_rotate<<<grid_for(n), 256, smem, s>>>(ws.V, n, m, ws.S, keep, ws.tmp, n);
     NSX_CUDA(cudaMemcpyAsync(ws.V, ws.tmp, sizeof(double) * n * keep, cudaMemcpyDeviceToDevice, s));
@@ -536,7 +554,6 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     // rotate Ritz vectors and their images; residuals in FP64
     NSX_CUDA(cudaMemcpyAsync(ws.S, S2.data(), sizeof(double) * nev * nev, cudaMemcpyHostToDevice, s));
     size_t smem = sizeof(double) * nev * nev;
-    NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1024)));
     count_launch();
     k_rotate<<<grid_for(n), 256, smem, s>>>(ws.tmp, n, nev, ws.S, nev, ws.V, n);
     count_launch();
@@ -555,8 +572,8 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     for (int c = 0; c < nev; ++c)
       if (res[c] <= tol && nconv == c) ++nconv;
   }
-  if (evecs_out) NSX_CUDA(cudaMemcpy(evecs_out, ws.tmp, sizeof(double) * n * nev, cudaMemcpyDeviceToHost));
-  NSX_CUDA(cudaDeviceSynchronize());
+  if (evecs_out) NSX_CUDA(cudaMemcpyAsync(evecs_out, ws.tmp, sizeof(double) * n * nev, cudaMemcpyDeviceToHost, s));
+  NSX_CUDA(cudaStreamSynchronize(s));
   if (rep) {
     std::memset(rep, 0, sizeof(*rep));
     rep->iterations = iters;

@@ -562,13 +562,20 @@ void upload_interaction(nsx_handle *h) {
     dev_refill<float>(d.hA32, h->A.hdense);
     dev_refill<float>(d.hB32, h->B.hdense);
   }
+  // copies from pageable memory may return before their DMA lands; work on non-blocking
+  // streams is not ordered after them
+  NSX_CUDA(cudaDeviceSynchronize());
+}
+
+cudaStream_t solve_stream(nsx_handle *h) {
+  if (!h->stream) NSX_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return h->stream;
 }
 
 void upload(nsx_handle *h) {
   NSX_CUDA(cudaSetDevice(h->device));
   if (h->max_anl > KA_MAXNL) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
-  d.rhoA = dev_copy<double>(h->A.vals);
   d.rhoB = dev_copy<double>(h->yrho);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
@@ -586,9 +593,9 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaMalloc(&d.xout, h->no_state * sizeof(double)));
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
-  for (size_t es : {sizeof(double), sizeof(float)}) {
-    (void)es;
-  }
+  // copies from pageable memory may return before their DMA lands; work on non-blocking
+  // streams (the caller's, or the handle's solve stream) is not ordered after them
+  NSX_CUDA(cudaDeviceSynchronize());
 }
 
 void ensure_precision(nsx_handle *h, int precision) {
@@ -603,7 +610,6 @@ void ensure_precision(nsx_handle *h, int precision) {
     if (!d.y32) {
       NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.z32, nz * sizeof(float)));
-      d.rhoA32 = dev_copy<float>(h->A.vals);
       d.rhoB32 = dev_copy<float>(h->yrho);
       d.hA32 = dev_copy<float>(h->A.hdense);
       d.hB32 = dev_copy<float>(h->B.hdense);
@@ -611,6 +617,7 @@ void ensure_precision(nsx_handle *h, int precision) {
       d.abar32 = dev_copy<float>(h->abar);
       NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
+      NSX_CUDA(cudaDeviceSynchronize());  // as in upload()
     }
   } else {
     fail(NSX_E_ARG, "unknown precision");
@@ -748,6 +755,8 @@ void release(nsx_handle *h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   h->ev0 = h->ev1 = nullptr;
+  if (h->stream) cudaStreamDestroy(h->stream);
+  h->stream = nullptr;
 }
 
 }  // namespace nsx

@@ -194,6 +194,7 @@ struct nsx_handle {
   double flops_like = 0, flops_y = 0, flops_mix = 0, flops_a = 0;
   nsx::DeviceBuffers d;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t stream = nullptr;   // non-blocking stream of nsx_solve / nsx_batch_solve (created on first use)
   // statistics
   int64_t launches = 0, matvecs = 0;
   int64_t stage_launches[NSX_STAGES] = {};
@@ -213,6 +214,7 @@ void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const do
                      const double *b_seg_vals, int64_t b_nvals);
 void upload(nsx_handle *h);
 void upload_interaction(nsx_handle *h);
+cudaStream_t solve_stream(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);

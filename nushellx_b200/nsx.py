@@ -88,6 +88,8 @@ SYMBOLS = {
     "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
     "nsx_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
+    "nsx_batch_solve": (C.c_int, [_p(C.c_void_p), C.c_int32, _p(Params), _p(_p(C.c_double)),
+                                  _p(_p(C.c_double)), _p(Report)]),
     "nsx_write_results": (C.c_int, [C.c_void_p, C.c_char_p, _p(C.c_double), _p(C.c_double), C.c_int32, C.c_int32,
                                     C.c_char_p, C.c_int32]),
     "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -311,6 +313,31 @@ class Solver:
         _check(self._lib.nsx_write_results(self._h, prefix.encode(), ev.ctypes.data_as(_p(C.c_double)),
                                            vv.ctypes.data_as(_p(C.c_double)), len(ev), int(iterations),
                                            intfile.encode(), int(T2)))
+
+    @staticmethod
+    def batch_solve(solvers, nev=10, tol=1e-6, precision=NSX_FP64, window=100, max_iter=3000, refine=False,
+                    want_vectors=False):
+        """Independent solves of distinct solvers at once (nsx_batch_solve); returns a list of
+        (eigenvalues, eigenvectors or None, report) in the order of `solvers`."""
+        lib = load_library()
+        n = len(solvers)
+        hs = (C.c_void_p * n)(*[s._h for s in solvers])
+        ps = (Params * n)()
+        for p in ps:
+            p.nev, p.tol, p.precision, p.window, p.keep = nev, tol, precision, window, 0
+            p.max_iter, p.pre_iter, p.seed, p.refine = max_iter, 2, 5, int(bool(refine))
+        evs = [np.zeros(nev) for _ in range(n)]
+        vecs = [np.zeros((nev, s.dim)) for s in solvers] if want_vectors else None
+        ev_ptrs = (_p(C.c_double) * n)(*[e.ctypes.data_as(_p(C.c_double)) for e in evs])
+        vec_ptrs = (_p(C.c_double) * n)(*[v.ctypes.data_as(_p(C.c_double)) for v in vecs]) if vecs else None
+        reps = (Report * n)()
+        _check(lib.nsx_batch_solve(hs, n, ps, ev_ptrs, vec_ptrs, reps))
+        out = []
+        for i in range(n):
+            r = reps[i].as_dict()
+            r["residual"] = [reps[i].residual[k] for k in range(min(nev, 64))]
+            out.append((evs[i], vecs[i] if vecs else None, r))
+        return out
 
     def stats_reset(self, timing=False):
         _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))
