@@ -332,8 +332,11 @@ def run_ours(args, world, rank, local):
         "max_abs_dE_vs_fp64_MeV": max(cmp["dE"]), "max_abs_dE_fp64_form_MeV": max(cmp["dE64"]),
         "eigenvalues_MeV": [float(v) for v in e32[0]],
         "matvecs": reps[-1]["matvecs"],
+        "matvecs_per_s": float(sum(r["matvecs"] for r in reps)) / (ms / 1e3 * args.steps),
         "matvec_ms": {k: v["ms"] / max(v["launches"], 1) for k, v in stages.items() if v["launches"]},
         "matvec_gflop": S.flops / 1e9,
+        "matvec_gflop_per_s": S.flops / 1e9 / (sum(v["ms"] / max(v["launches"], 1) for v in stages.values()
+                                                   if v["launches"]) * 1e-3),
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
                      "algorithmic_bytes_per_launch": d["bytes"]},
