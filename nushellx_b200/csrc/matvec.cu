@@ -388,11 +388,40 @@ __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, cons
 // through shared memory and the tile adds its result to the output with atomic
 // adds (K ranges of one slab are separate tiles; the like-particle stage wrote
 // the output first).
+// Tile shape (compile-time; the defaults are the fastest of a sweep on B200 at fp 6p+6n,
+// 2-4 stages x 8-64 rows x row groups of 8/16 x 1 or 4 groups per pass): stacked rows per
+// stage KS, output rows per register group RG, row groups sharing one pass over the K range
+// GPP (1: the 4 warps split the stacked rows; 4: the warps take different row groups, so a
+// slab with many rows does not re-read its Zbar tile from HBM), and the pipeline depth.
+// Measured: FP32 0.76 ms (KS 32, RG 16, GPP 1), FP64 1.59 ms (KS 16, RG 8, GPP 4).
+#ifndef KA_KS32
+#define KA_KS32 32
+#endif
+#ifndef KA_RG32
+#define KA_RG32 16
+#endif
+#ifndef KA_GPP32
+#define KA_GPP32 1
+#endif
+#ifndef KA_KS64
+#define KA_KS64 16
+#endif
+#ifndef KA_RG64
+#define KA_RG64 8
+#endif
+#ifndef KA_GPP64
+#define KA_GPP64 4
+#endif
+#ifndef KA_NSTAGE
+#define KA_NSTAGE 2
+#endif
 template <typename T> struct KaCfg;
-template <> struct KaCfg<float> { static constexpr int KS = 16, RG = 16; };
-template <> struct KaCfg<double> { static constexpr int KS = 8, RG = 8; };
-constexpr int KA_STAGES = 3;
+template <> struct KaCfg<float> { static constexpr int KS = KA_KS32, RG = KA_RG32, GPP = KA_GPP32; };
+template <> struct KaCfg<double> { static constexpr int KS = KA_KS64, RG = KA_RG64, GPP = KA_GPP64; };
+static_assert(KA_GPP32 >= 1 && KA_GPP32 <= 4 && KA_GPP64 >= 1 && KA_GPP64 <= 4, "1 to 4 row groups per pass");
+constexpr int KA_STAGES = KA_NSTAGE;
 constexpr int KA_MAXNL = 64;
+static_assert(KA_RG32 % 4 == 0 && KA_RG64 % 4 == 0, "row groups of whole 4-row vectors");
 
 __device__ __forceinline__ void ka_cp16(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -421,11 +450,11 @@ struct KaSmem {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
+__global__ void __launch_bounds__(128, 5) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
                                            const T *__restrict__ Zb, T *__restrict__ out) {
   constexpr int KS = KaCfg<T>::KS, RG = KaCfg<T>::RG, TC = KA_TILE_COLS;
   constexpr int CPR = TC * (int)sizeof(T) / 16;                  // 16-byte chunks per Zbar row
-  __shared__ __align__(16) unsigned char raw[KaSmem<T>::bytes];
+  extern __shared__ __align__(16) unsigned char raw[];            // KaSmem<T>::bytes
   T *zs = reinterpret_cast<T *>(raw);                             // [KA_STAGES][KS][TC]
   T *as = zs + (size_t)KA_STAGES * KS * TC;                       // [KA_STAGES][KS * nlp]
   T *red = reinterpret_cast<T *>(raw);                            // [4][RG][TC] after a pass
@@ -451,13 +480,23 @@ __global__ void __launch_bounds__(128) k_a(const ATile *__restrict__ tiles, cons
     for (int e = tid; e < na; e += 128) ka_cp16(ab + e * (16 / (int)sizeof(T)), asrc + e * (16 / (int)sizeof(T)));
   };
 
-  for (int l0 = 0; l0 < nl; l0 += RG) {
+  // Row groups of RG output rows: up to GPP per pass over the K range, spread over the
+  // warps (1 group: 4 warps split K; 2: 2 warps each; 3-4: one warp each), so that each
+  // Zbar tile crosses HBM once per GPP row groups.
+  const int ngr = (nl + RG - 1) / RG;
+  constexpr int GPP = KaCfg<T>::GPP;
+  for (int gp0 = 0; gp0 < ngr; gp0 += GPP) {
+    const int npg = min(GPP, ngr - gp0);
+    const int wpg = npg == 1 ? 4 : (npg == 2 ? 2 : 1);
+    const int gi = warp / wpg, ks = warp - gi * wpg;
+    const bool active = gi < npg;
+    const int l0 = (gp0 + (active ? gi : 0)) * RG;
+    const int ng = active ? min(RG, nlp - l0) / 4 : 0;            // groups of 4 rows with Abar entries
     T acc[RG][4];
 #pragma unroll
     for (int i = 0; i < RG; ++i)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[i][c] = T(0);
-    const int ng = min(RG, nlp - l0) / 4;                        // groups of 4 rows with Abar entries
 #pragma unroll
     for (int s = 0; s < KA_STAGES - 1; ++s) {
       if (s < nchunk) load(s, s);
@@ -472,37 +511,41 @@ __global__ void __launch_bounds__(128) k_a(const ATile *__restrict__ tiles, cons
       const int kc = min(KS, t.k_end - (t.k_begin + c * KS));
       const T *zb = zs + (size_t)b * KS * TC + 4 * lane;
       const T *ab = as + (size_t)b * KS * KA_MAXNL + l0;
-      for (int r = warp; r < kc; r += 4) {
-        T z[4];
-        ka_ld4(zb + r * TC, z);
-        const T *ar = ab + r * nlp;
+      if (active) {
+        for (int r = ks; r < kc; r += wpg) {
+          T z[4];
+          ka_ld4(zb + r * TC, z);
+          const T *ar = ab + r * nlp;
 #pragma unroll
-        for (int g = 0; g < RG / 4; ++g) {
-          if (g < ng) {
-            T a[4];
-            ka_ld4(ar + 4 * g, a);
+          for (int g = 0; g < RG / 4; ++g) {
+            if (g < ng) {
+              T a[4];
+              ka_ld4(ar + 4 * g, a);
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+              for (int i = 0; i < 4; ++i)
 #pragma unroll
-              for (int cc = 0; cc < 4; ++cc) acc[4 * g + i][cc] = fma(a[i], z[cc], acc[4 * g + i][cc]);
+                for (int cc = 0; cc < 4; ++cc) acc[4 * g + i][cc] = fma(a[i], z[cc], acc[4 * g + i][cc]);
+            }
           }
         }
       }
       __syncthreads();
     }
     ka_wait<0>();
-    // add the 4 warps' partial sums and the result to the output
+    // add the K-slot warps' partial sums of each row group; the result goes to the output
 #pragma unroll
     for (int i = 0; i < RG; ++i)
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) red[((size_t)warp * RG + i) * TC + 4 * lane + cc] = acc[i][cc];
     __syncthreads();
     if (tid < t.ncols) {
-      for (int i = 0; i < RG && l0 + i < nl; ++i) {
-        T v = red[(size_t)i * TC + tid];
-#pragma unroll
-        for (int w = 1; w < 4; ++w) v += red[((size_t)w * RG + i) * TC + tid];
-        atomicAdd(out + t.out + (l0 + i) + (int64_t)t.ld * tid, v);
+      for (int gg = 0; gg < npg; ++gg) {
+        const int lg = (gp0 + gg) * RG;
+        for (int i = 0; i < RG && lg + i < nl; ++i) {
+          T v = T(0);
+          for (int w = 0; w < wpg; ++w) v += red[((size_t)(gg * wpg + w) * RG + i) * TC + tid];
+          atomicAdd(out + t.out + (lg + i) + (int64_t)t.ld * tid, v);
+        }
       }
     }
     __syncthreads();
@@ -593,6 +636,9 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaMalloc(&d.xout, h->no_state * sizeof(double)));
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
+  // k_a's shared-memory cap: the same constant on every call (harmless to repeat)
+  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<float>::bytes));
+  NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<double>::bytes));
   // copies from pageable memory may return before their DMA lands; work on non-blocking
   // streams (the caller's, or the handle's solve stream) is not ordered after them
   NSX_CUDA(cudaDeviceSynchronize());
@@ -702,7 +748,7 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T
   }
   if (!h->atiles.empty()) {
     StageScope sc(h, 3, s);
-    k_a<T><<<(unsigned)h->atiles.size(), 128, 0, s>>>(d.atiles, abar, Z, out);
+    k_a<T><<<(unsigned)h->atiles.size(), 128, KaSmem<T>::bytes, s>>>(d.atiles, abar, Z, out);
   }
   NSX_CUDA(cudaGetLastError());
 }
