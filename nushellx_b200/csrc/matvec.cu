@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(128, 5) k_a(const ATile *__restrict__ tiles, c
   const int ngr = (nl + RG - 1) / RG;
   constexpr int GPP = KaCfg<T>::GPP;
   for (int gp0 = 0; gp0 < ngr; gp0 += GPP) {
-    const int npg = min(GPP, ngr - gp0);
+    const int npg = GPP == 1 ? 1 : min(GPP, ngr - gp0);          // a constant when GPP == 1
     const int wpg = npg == 1 ? 4 : (npg == 2 ? 2 : 1);
     const int gi = warp / wpg, ks = warp - gi * wpg;
     const bool active = gi < npg;
@@ -512,22 +512,29 @@ __global__ void __launch_bounds__(128, 5) k_a(const ATile *__restrict__ tiles, c
       const T *zb = zs + (size_t)b * KS * TC + 4 * lane;
       const T *ab = as + (size_t)b * KS * KA_MAXNL + l0;
       if (active) {
-        for (int r = ks; r < kc; r += wpg) {
-          T z[4];
-          ka_ld4(zb + r * TC, z);
-          const T *ar = ab + r * nlp;
+        // the stacked rows of this warp: ks, ks + wpg, ... (the stride as a constant)
+        auto rows = [&](auto stride) {
+          constexpr int WS = decltype(stride)::value;
+          for (int r = ks; r < kc; r += WS) {
+            T z[4];
+            ka_ld4(zb + r * TC, z);
+            const T *ar = ab + r * nlp;
 #pragma unroll
-          for (int g = 0; g < RG / 4; ++g) {
-            if (g < ng) {
-              T a[4];
-              ka_ld4(ar + 4 * g, a);
+            for (int g = 0; g < RG / 4; ++g) {
+              if (g < ng) {
+                T a[4];
+                ka_ld4(ar + 4 * g, a);
 #pragma unroll
-              for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) acc[4 * g + i][cc] = fma(a[i], z[cc], acc[4 * g + i][cc]);
+                  for (int cc = 0; cc < 4; ++cc) acc[4 * g + i][cc] = fma(a[i], z[cc], acc[4 * g + i][cc]);
+              }
             }
           }
-        }
+        };
+        if (wpg == 4) rows(std::integral_constant<int, 4>());
+        else if (wpg == 2) rows(std::integral_constant<int, 2>());
+        else rows(std::integral_constant<int, 1>());
       }
       __syncthreads();
     }
