@@ -415,6 +415,9 @@ __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, cons
 #ifndef KA_NSTAGE
 #define KA_NSTAGE 2
 #endif
+#ifndef KA_MINB    // resident CTAs per SM the register budget is sized for (shared memory allows 4)
+#define KA_MINB 4
+#endif
 template <typename T> struct KaCfg;
 template <> struct KaCfg<float> { static constexpr int KS = KA_KS32, RG = KA_RG32, GPP = KA_GPP32; };
 template <> struct KaCfg<double> { static constexpr int KS = KA_KS64, RG = KA_RG64, GPP = KA_GPP64; };
@@ -450,7 +453,7 @@ struct KaSmem {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128, 5) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
+__global__ void __launch_bounds__(128, KA_MINB) k_a(const ATile *__restrict__ tiles, const T *__restrict__ Abar,
                                            const T *__restrict__ Zb, T *__restrict__ out) {
   constexpr int KS = KaCfg<T>::KS, RG = KaCfg<T>::RG, TC = KA_TILE_COLS;
   constexpr int CPR = TC * (int)sizeof(T) / 16;                  // 16-byte chunks per Zbar row

@@ -136,6 +136,7 @@ class LearnedStart:
         self.net.params = m["params"]
         self.comp = Compressor(m["desc"], m["shapes"], int(m["dim"]), m["rank"])
         self.dim = int(m["dim"])
+        self._rand = {}   # (solver dimension, seed) -> normalised standard random vector
 
     def projections(self, lam):
         x = np.asarray(lam, dtype=np.float32).reshape(1, -1) / self.lam_scale
@@ -150,8 +151,11 @@ class LearnedStart:
         n0 = np.linalg.norm(x0)
         if not np.isfinite(n0) or n0 == 0.0:
             return None
-        r = standard_start(S, seed)
-        return x0 / n0 + beta * r / np.linalg.norm(r)
+        key = (S.dim, seed)
+        if key not in self._rand:   # the same seeded vector for every variant of the space
+            r = standard_start(S, seed)
+            self._rand[key] = r / np.linalg.norm(r)
+        return x0 / n0 + beta * self._rand[key]
 
     def close(self):
         self.net.close()
