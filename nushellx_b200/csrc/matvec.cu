@@ -720,7 +720,7 @@ void flush_stage_events(nsx_handle *h) {
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]) {
   const double es = precision == NSX_FP64 ? 8.0 : 4.0;
   const double n = (double)h->no_state;
-  double rhoA = (double)h->A.vals.size(), rhoB = (double)h->B.vals.size();
+  const double rhoB = (double)h->B.vals.size();
   double hd = (double)(h->A.hdense.size() + h->B.hdense.size());
   const double y = (double)h->y_elems, z = (double)h->z_elems;
   bytes[0] = es * (2.0 * n + hd);                         // C in, out written, dense H
@@ -736,10 +736,9 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAG
 }
 
 template <typename T>
-static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoA, const T *rhoB, const T *hA, const T *hB,
-                       const T *w, const T *abar, T *Y, T *Z, cudaStream_t s) {
+static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoB, const T *hA, const T *hB, const T *w,
+                       const T *abar, T *Y, T *Z, cudaStream_t s) {
   auto &d = h->d;
-  (void)rhoA;
   if (!h->ltiles.empty()) {
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
@@ -769,7 +768,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
   h->matvecs++;
   h->last_precision = precision;
   if (precision == NSX_FP64) {
-    run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, d.y64, d.z64, s);
+    run_stages<double>(h, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, d.y64, d.z64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -777,7 +776,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       StageScope sc(h, 4, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float>(h, d.x32, d.o32, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32, d.y32, d.z32, s);
+    run_stages<float>(h, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32, d.y32, d.z32, s);
     {
       StageScope sc(h, 4, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
@@ -792,12 +791,12 @@ void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double 
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = NSX_FP64;
-  run_stages<double>(h, x, y, d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
+  run_stages<double>(h, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
 }
 
 void release(nsx_handle *h) {
   auto &d = h->d;
-  void *ptrs[] = {d.rhoA, d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoA32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
+  void *ptrs[] = {d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
                   d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zops, d.atiles, d.ltiles,
                   d.y64, d.z64, d.y32, d.z32, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)

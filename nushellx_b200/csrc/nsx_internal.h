@@ -143,8 +143,9 @@ struct LTile {
 
 struct DeviceBuffers {
   // FP64 operator data
-  double *rhoA = nullptr, *rhoB = nullptr, *hA = nullptr, *hB = nullptr, *w = nullptr;
-  float *rhoA32 = nullptr, *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr, *w32 = nullptr;
+  // rhoB: the padded neutron densities of the Y stage (the proton densities live in abar)
+  double *rhoB = nullptr, *hA = nullptr, *hB = nullptr, *w = nullptr;
+  float *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr, *w32 = nullptr;
   double *abar = nullptr;
   float *abar32 = nullptr;
   YGroup *ygroups = nullptr;

@@ -53,3 +53,14 @@ def racah_weight(J2al, J2bl, J2ar, J2br, J2, lam2):
         return 0.0
     ph = -1.0 if ((J2al + J2br - J2 - lam2) // 2) % 2 else 1.0
     return ph * w * np.sqrt(lam2 + 1.0)
+
+
+def op_order(vlam):
+    """The order of the pn multipole operators in nsx_problem.op_keys (sorted labels)."""
+    return sorted(vlam)
+
+
+def op_values(vlam, order):
+    """Multipole values in a given operator order (0 for labels the dict does not hold)."""
+    import numpy as np
+    return np.array([vlam.get(k, 0.0) for k in order], dtype=np.float64)

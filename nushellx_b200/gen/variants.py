@@ -10,9 +10,8 @@ them through ``Solver.set_interaction`` (nsx_set_interaction) without re-plannin
 import numpy as np
 
 from .space import gaussian_interaction
-from .pnint import multipole_pn
+from .pnint import multipole_pn, op_order, op_values
 from .writer import segment_arrays
-from ..nsx import op_order, op_values
 
 
 class InteractionFamily:

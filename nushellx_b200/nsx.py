@@ -176,19 +176,10 @@ def _species_struct(keep, S, dens, segs):
     return s
 
 
-def op_order(vlam):
-    """The order of the pn multipole operators in nsx_problem.op_keys (sorted labels)."""
-    return sorted(vlam)
-
-
-def op_values(vlam, order):
-    """Multipole values in a given operator order (0 for labels the dict does not hold)."""
-    return np.array([vlam.get(k, 0.0) for k in order], dtype=np.float64)
-
-
 def build_problem_struct(P):
     """nsx_problem for an in-memory generated problem; returns (struct, arrays to keep alive)."""
     from .gen.writer import density_arrays, segment_arrays
+    from .gen.pnint import op_order, op_values
     keep = []
     prob = Problem()
     prob.J2, prob.parity = P.J2, P.parity

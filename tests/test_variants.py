@@ -29,7 +29,7 @@ def _direct(P, inter):
 @pytest.mark.parametrize("name", ["sd_2p2n_0", "sd_2p2n_2"])
 def test_family_arrays_match_direct_generation(name):
     from nushellx_b200.gen.writer import segment_arrays
-    from nushellx_b200.nsx import op_values
+    from nushellx_b200.gen.pnint import op_values
     P = make_problem(name)
     fam = _family(name)
     op, a, b = fam.arrays(LAM)
