@@ -3,18 +3,20 @@
 // The reference computes the product as multiplyx (pn), multiplya (pp) and
 // multiplyb (nn) in src/NuLnz/NuCoreX.f90:76-226 with axpy loops over density
 // sub-blocks (src/NuCommonX/NuCommonX.f90:745-919, 1009-1104).  Here it is
-// four stream-ordered kernels; every output element is owned by one thread
-// block (no atomics, no per-thread copies of the vector):
+// four stream-ordered kernels, with no per-thread copies of the vector:
 //
 //   k_like : out_b = H_pp(Ja) C_b + C_b H_nn(Jb)                  (dense tiled GEMM)
 //   k_y    : Y_(h,k) = C_h rho_k^T for every (input block h, neutron density k)
 //            the pn table uses -- once, where the reference recomputes it for
-//            every proton operator; row-major d_ar x d_bl
+//            every proton operator; row-major d_ar x d_bl.  FP32 pieces on the
+//            tensor cores (mma.sync TF32 with the 3xTF32 split), FP64 SIMT
 //   k_z    : Z_a[P_r rows] = sum_s w_(a,s) Y_s[P_r rows] for the proton operators
 //            of each (output block, J_ar, lam) group, written as rows of the
 //            stacked operand Zbar of the output slab (block, P_l) a leads to
 //   k_a    : out[P_l rows] += Abar Zbar, Abar = the slab's proton density blocks
-//            side by side: one long-K product per output slab, no mixing
+//            side by side: one long-K product per output slab, streamed through
+//            a cp.async shared-memory pipeline; slabs longer than 512 stacked rows
+//            are split and their partial sums added atomically
 //
 // Each intermediate (Y, Zbar) is written once and read once, in row streams.
 // Templated on the contraction type: double (the FP64 form) or float (the FP32

@@ -68,6 +68,34 @@ def test_subblocks_tile_the_parity_mask_and_compression_inverts():
     assert np.allclose(comp.compress(-g), w)          # sign convention
 
 
+def test_compression_from_a_training_set():
+    """Kept sub-blocks = largest mean weight over the training states; shapes = dominant
+    singular vectors (independent of each state's overall sign); projections sign-aligned."""
+    import torch
+    from nushellx_b200.learned.compress import SubBlocks, Compressor
+    P = make_problem("fp_4p4n_0")
+    sub = SubBlocks(P)
+    rng = np.random.default_rng(8)
+    base = rng.standard_normal(P.no_state) * P.lcoef
+    base /= np.linalg.norm(base)
+    G = np.stack([(1 if i % 2 else -1) * (base * (1 + 0.05 * rng.standard_normal())
+                                          + 1e-3 * rng.standard_normal(P.no_state) * P.lcoef) for i in range(24)])
+    comp = Compressor.from_training(sub, torch.tensor(G, dtype=torch.float32), 64)
+    assert comp.K == 64
+    # the kept sub-blocks are the 64 heaviest by mean weight
+    e = np.mean([sub.norms(g) ** 2 for g in G], axis=0)
+    kept = {tuple(d) for d in comp.desc}
+    heaviest = {tuple(sub.desc[i]) for i in np.argsort(-e)[:64]}
+    assert kept == heaviest
+    # unit shapes, one per kept sub-block
+    assert np.allclose(np.sqrt(np.add.reduceat(comp.shapes ** 2, comp.start[:-1])), 1.0)
+    W = np.stack([comp.compress(g) for g in G])
+    lead = comp.rank[0]
+    assert np.all(W[:, lead] > 0)                      # alternating overall signs are aligned
+    assert np.corrcoef(W)[0, 1:].min() > 0.99           # the same state up to noise
+    assert np.allclose(comp.compress(comp.decompress(W[3])), W[3])
+
+
 @pytest.mark.gpu
 def test_network_forward_and_gradients_match_the_oracle():
     from nushellx_b200.build import build
