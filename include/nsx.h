@@ -183,13 +183,14 @@ int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *par
 
 /* Write eigenpairs (evals[nev], evecs[nev][no_state], e.g. from nsx_solve) in the
  * reference's output files, as NuTRL leaves them for NuVec (src/NuLnz/NuCoreX.f90:526-533,
- * 280-281; src/NuVec/NuVec.f90:120-131, 285-286, 298-321):
+ * 280-281; src/NuVec/NuVec.f90:120-131, 182, 281, 285-286, 298-321):
  *   <prefix>.abz  thick-restart form, 4 records: isave = nev, alpha = E, betat = 0,
  *                 matrix = diag(E); imax = iterations, no_level = nev, tt, no_state, basd,
  *                 count = 2, no_keep = no_conv = nev, first_iter, second_iter, noiter;
  *                 bas; alpha_copy, betat(isave+1), indx
  *   <prefix>.trl  one FP32 direct-access record of no_state values per eigenvector
  *   <prefix>.lev  header (intfile, 2J and 2T = T2) and the levels as 5(f10.3,a1)
+ *   <prefix>.xvc  NuVec's eigenvector file: (no_state, nev), then (E_i, vector_i) in FP32
  * NuVec's reconstruction from these files returns exactly the given eigenpairs.
  * The reference names prefix Nucleus // file_code(J2/2, no_cA, no_cB). */
 int nsx_write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs,

@@ -4,8 +4,9 @@
 // .oph pn interaction, the .spe header with renorm and no_level, and the like-particle
 // .sgt/.mat files found by file code), finds the no_level lowest states with the GPU
 // solver (FP32 H.v + FP64 thick-restart Lanczos + FP64 Rayleigh-Ritz by default) and
-// writes <nucleus><file_code(J2/2, nprot, nneut)>.abz / .trl / .lev in the reference's
-// formats, which NuVec reads (src/NuLnz/NuCoreX.f90:526-533, src/NuVec/NuVec.f90:120-131).
+// writes <nucleus><file_code(J2/2, nprot, nneut)>.abz / .trl (what NuVec reads) and
+// .lev / .xvc (what NuVec writes) in the reference's formats (src/NuLnz/NuCoreX.f90:526-533,
+// src/NuVec/NuVec.f90:120-131, 182, 281).
 // Like the reference it stops with a message and a non-zero exit status on failure.
 //
 // The reference's lanc takes its file names from NuShellX's interactive setup
@@ -107,7 +108,7 @@ int main(int argc, char **argv) {
   std::printf(" dimension %lld, %d Lanczos steps, %d H.v, %.3f s (H.v %.3f s)\n", (long long)n, rep.iterations,
               rep.matvecs, rep.seconds, rep.matvec_seconds);
   for (int i = 0; i < nev; ++i) std::printf("%10.3f%s", ev[i], (i % 5 == 4 || i == nev - 1) ? "\n" : "");
-  std::printf(" wrote %s.abz %s.trl %s.lev\n", prefix.c_str(), prefix.c_str(), prefix.c_str());
+  std::printf(" wrote %s.abz .trl .lev .xvc\n", prefix.c_str());
   nsx_destroy(h);
   return 0;
 }

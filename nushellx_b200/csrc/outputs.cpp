@@ -14,6 +14,9 @@
 //   <prefix>.lev  formatted: the header NuVec's output_results writes after its program
 //                 banner (NuVec.f90:298-321) and the levels as 5(f10.3,a1), each with its
 //                 parity character (NuVec.f90:239-241, 285-286)
+//   <prefix>.xvc  unformatted sequential, as NuVec writes its eigenvectors (NuVec.f90:182,
+//                 281): record 1: no_state, number of levels (i4); then one record per
+//                 level: energy (r4), vector(1:no_state) (r4)
 //
 // The basis written is the converged Ritz vectors themselves (isave = nev), with
 // matrix = diag(E), alpha = E, betat = 0 and count = 2: NuVec's reconstruction
@@ -50,6 +53,7 @@ struct RecordWriter {
     buf.insert(buf.end(), q, q + n);
   }
   void end_record() {
+    if (buf.size() > 0x7fffffffu) fail(NSX_E_ARG, "record longer than a 4-byte Fortran record marker can state");
     const uint32_t n = (uint32_t)buf.size();
     if (std::fwrite(&n, 4, 1, f) != 1 || (n && std::fwrite(buf.data(), 1, n, f) != n) || std::fwrite(&n, 4, 1, f) != 1)
       fail(NSX_E_IO, "write failed");
@@ -123,6 +127,19 @@ void write_results(const nsx_handle *h, const char *prefix, const double *evals,
       }
     }
     std::fclose(f);
+  }
+  // .xvc
+  {
+    RecordWriter w(base + ".xvc");
+    w.put<int32_t>((int32_t)n);
+    w.put<int32_t>(nev);
+    w.end_record();
+    for (int i = 0; i < nev; ++i) {
+      w.put<float>((float)evals[i]);
+      const double *v = evecs + (size_t)i * n;
+      for (int64_t k = 0; k < n; ++k) w.put<float>((float)v[k]);
+      w.end_record();
+    }
   }
   // .lev
   {

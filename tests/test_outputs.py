@@ -80,6 +80,15 @@ def test_write_results_reads_back_as_nuvec_does(name, tmp_path):
         assert np.abs(s * psi[i] - vecs[i]).max() <= 1e-6 * np.abs(vecs[i]).max()
     assert np.allclose(lv, ev, atol=6e-4)
     assert set(par) == {"+"}          # J^pi = 0+ in the positive-parity sector
+    # .xvc, as NuVec writes it: (no_state, levels), then (E, vector) per level in FP32
+    recs = read_records(prefix + ".xvc")
+    assert struct.unpack("<ii", recs[0]) == (S.dim, nev) and len(recs) == nev + 1
+    for i in range(nev):
+        assert len(recs[i + 1]) == 4 * (1 + S.dim)
+        e = struct.unpack_from("<f", recs[i + 1], 0)[0]
+        v = np.frombuffer(recs[i + 1], dtype="<f4", offset=4)
+        assert abs(e - ev[i]) <= 1e-6 * max(1.0, abs(ev[i]))
+        assert np.abs(v - vecs[i]).max() <= 1e-6 * np.abs(vecs[i]).max()
     S.close()
 
 
