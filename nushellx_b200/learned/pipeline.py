@@ -33,7 +33,7 @@ NPERTURB = 8
 PERTURB_SEED0 = 1000
 
 
-def _solver_and_family(workload):
+def solver_and_family(workload):
     from ..gen.space import WORKLOADS
     from ..gen.problem import JProblem
     from ..gen.variants import InteractionFamily
@@ -63,7 +63,7 @@ def sweep(workload, nvar, seed, K, out, ntrain=None, tol=1e-5, log=print):
     from ..gen.variants import sample_lambdas
     ntrain = nvar if ntrain is None else ntrain
     t0 = time.time()
-    P, fam, S = _solver_and_family(workload)
+    P, fam, S = solver_and_family(workload)
     log(f"setup {time.time() - t0:.1f} s, dim {S.dim}")
     lams = sample_lambdas(nvar, NPERTURB, seed, LAM_SCALE)
     G = torch.zeros((nvar, S.dim), dtype=torch.float32, device="cuda")   # ground states, kept in HBM
@@ -204,7 +204,7 @@ def main():
     else:
         d = np.load(a.data)
         learned = LearnedStart(a.model)
-        P, fam, S = _solver_and_family(learned.workload)
+        P, fam, S = solver_and_family(learned.workload)
         ntrain = int(np.load(a.model)["ntrain"])
         rows = compare(S, fam, learned, d["lams"][ntrain:ntrain + a.count], beta=a.beta)
         it_s = np.mean([r["iter_standard"] for r in rows])

@@ -137,7 +137,7 @@ def test_learned_start_saves_iterations_on_held_out_variants(tmp_path):
     stats = L.train(data, 48, model, width=256, steps=1500, lr=2e-3, log=lambda *a: None)
     assert stats["err_test"] < stats["err_mean_predictor"]   # the network beats predicting the mean
     learned = L.LearnedStart(model)
-    P, fam, S = L._solver_and_family("fp_4p4n_0")
+    P, fam, S = L.solver_and_family("fp_4p4n_0")
     lams = np.load(data)["lams"][48:60]
     rows = L.compare(S, fam, learned, lams, nev=10, tol=1e-6, log=lambda *a: None)
     it_std = np.mean([r["iter_standard"] for r in rows])
@@ -146,7 +146,7 @@ def test_learned_start_saves_iterations_on_held_out_variants(tmp_path):
     assert it_l < it_std
     assert max(r["max_dE"] for r in rows) < 1e-5
     # fallback: a model for another vector space yields no start vector
-    S2 = L._solver_and_family("sd_2p2n_0")[2]
+    S2 = L.solver_and_family("sd_2p2n_0")[2]
     assert learned.start_vector(S2, lams[0]) is None
     S.close()
     S2.close()
