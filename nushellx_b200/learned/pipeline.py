@@ -34,6 +34,8 @@ PERTURB_SEED0 = 1000
 
 
 def solver_and_family(workload):
+    """(problem, interaction family with the 8 seeded perturbations, solver handle on cuda) of a
+    named workload; variants are loaded into the handle with Solver.set_interaction."""
     from ..gen.space import WORKLOADS
     from ..gen.problem import JProblem
     from ..gen.variants import InteractionFamily
