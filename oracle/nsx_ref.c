@@ -422,11 +422,14 @@ static double dot44(const float *a, const float *b, int64_t n) {
 
 /* Standard Lanczos (NuCoreX.f90:595-707) for nsteps iterations after npre power
  * pre-iterations, vectors in RAM.  Writes alpha/beta (nsteps each) and returns
- * the wall seconds spent in the steps (pre-iterations included in pre_seconds). */
+ * the wall seconds spent in the steps (pre-iterations in pre_seconds; the part of
+ * the steps spent in the Gram-Schmidt loop against the stored vectors in
+ * cgs_seconds, so that its cost per stored vector is measured, not inferred). */
 double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *alpha, double *beta,
-                   double *pre_seconds) {
+                   double *pre_seconds, double *cgs_seconds) {
   const int64_t N = h->no_state;
   float *V = malloc(sizeof(float) * N * (size_t)(nsteps + 1));
+  memset(V, 0, sizeof(float) * N * (size_t)(nsteps + 1));  /* first touch outside the timed steps */
   float *L = malloc(sizeof(float) * N), *R = malloc(sizeof(float) * N), *Tv = malloc(sizeof(float) * N);
   uint64_t z = seed ? seed : 5;
   for (int64_t i = 0; i < N; ++i) {
@@ -446,6 +449,7 @@ double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *a
   if (pre_seconds) *pre_seconds = t1 - t0;
   memcpy(V, R, sizeof(float) * N);
   float b = 0;
+  double tcgs = 0;
   for (int it = 0; it < nsteps; ++it) {
     ref_matvec(h, R, L);
     if (it) {
@@ -457,6 +461,7 @@ double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *a
 #pragma omp parallel for
     for (int64_t i = 0; i < N; ++i) L[i] -= a * R[i];
     /* lnzort: classical Gram-Schmidt against all stored vectors (NuCoreX.f90:766-778) */
+    const double tg0 = omp_get_wtime();
     memcpy(R, L, sizeof(float) * N);
     for (int j = 0; j <= it; ++j) {
       const float *vj = V + (size_t)j * N;
@@ -468,6 +473,7 @@ double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *a
 #pragma omp parallel for
       for (int64_t i = 0; i < N; ++i) L[i] -= o * vj[i];
     }
+    tcgs += omp_get_wtime() - tg0;
     b = (float)sqrt(dot44(L, L, N));
     alpha[it] = a;
     beta[it] = b;
@@ -476,6 +482,7 @@ double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *a
     memcpy(V + (size_t)(it + 1) * N, R, sizeof(float) * N);
   }
   double t2 = omp_get_wtime();
+  if (cgs_seconds) *cgs_seconds = tcgs;
   free(V); free(L); free(R); free(Tv);
   return t2 - t1;
 }

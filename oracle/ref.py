@@ -24,7 +24,7 @@ def lib():
         L.ref_matvec.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.ref_lanczos.restype = C.c_double
         L.ref_lanczos.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double),
-                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ref_destroy.restype = None
         L.ref_destroy.argtypes = [C.c_void_p]
         _lib = L
@@ -48,12 +48,15 @@ class RefSolver:
         return y
 
     def lanczos(self, npre, nsteps, seed=5):
+        """(seconds of the steps, seconds of the pre-iterations, seconds of the steps spent in
+        Gram-Schmidt against the stored vectors, alpha, beta)."""
         a = np.zeros(max(nsteps, 1))
         b = np.zeros(max(nsteps, 1))
         pre = C.c_double(0)
+        cgs = C.c_double(0)
         t = lib().ref_lanczos(self._h, npre, nsteps, seed, a.ctypes.data_as(C.POINTER(C.c_double)),
-                              b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pre))
-        return t, pre.value, a[:nsteps], b[:nsteps]
+                              b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pre), C.byref(cgs))
+        return t, pre.value, cgs.value, a[:nsteps], b[:nsteps]
 
     def close(self):
         if self._h:
