@@ -106,7 +106,11 @@ typedef struct nsx_report {
 typedef struct nsx_handle nsx_handle;
 
 /* Build a solver handle from host arrays.  The library copies what it needs
- * to the device; the caller keeps ownership of the host buffers. */
+ * to the device; the caller keeps ownership of the host buffers.  With device < 0
+ * the handle is plan only: no device memory and no CUDA call, for inspecting a
+ * problem (nsx_dim, nsx_blocks, nsx_lcoef, nsx_matvec_flops), loading new
+ * interactions and writing result files on a host without a GPU; H.v and solves
+ * on it fail with NSX_E_ARG (NSX_E_CUDA from nsx_matvec_noalloc). */
 int nsx_create(const nsx_problem *prob, int device, nsx_handle **out);
 
 /* The reference's input file set (src/NuLnz/NuCoreX.f90:1659-1670, 1216-1319).

@@ -22,6 +22,12 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals, double *evecs, nsx
 std::shared_ptr<void> load_files(const nsx_files *f, nsx_problem *p);
 int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 
+// Device calls on a handle: a plan-only handle (created with device < 0) has no device data.
+static void require_device(const nsx_handle *h) {
+  if (h->device < 0) fail(NSX_E_ARG, "the handle was created without a device (plan only)");
+  NSX_CUDA(cudaSetDevice(h->device));
+}
+
 template <typename F>
 static int guarded(F &&f) {
   try {
@@ -62,7 +68,11 @@ int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
   }
   int rc = guarded([&] {
     if (!prob) fail(NSX_E_ARG, "null problem");
-    h->device = device;
+    h->device = device < 0 ? -1 : device;
+    if (device < 0) {   // plan only: no CUDA call at all
+      build_plan(h, prob);
+      return;
+    }
     NSX_CUDA(cudaSetDevice(device));
     build_plan(h, prob);
     upload(h);
@@ -93,7 +103,7 @@ int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const
   return guarded([&] {
     if (!h) fail(NSX_E_ARG, "null handle");
     set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals);
-    upload_interaction(h);
+    if (h->device >= 0) upload_interaction(h);
   });
 }
 
@@ -105,6 +115,7 @@ int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *par
     std::vector<nsx_handle *> hs(handles, handles + n);
     for (int i = 0; i < n; ++i) {
       if (!hs[i] || !evals[i]) fail(NSX_E_ARG, "null handle or eigenvalue array for problem " + std::to_string(i));
+      if (hs[i]->device < 0) fail(NSX_E_ARG, "problem " + std::to_string(i) + ": the handle was created without a device (plan only)");
       for (int j = 0; j < i; ++j)
         if (hs[j] == hs[i]) fail(NSX_E_ARG, "the same handle is listed twice (problems " + std::to_string(j) +
                                                 " and " + std::to_string(i) + ")");
@@ -178,7 +189,7 @@ int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, voi
   return guarded([&] {
     if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
     if (x == y) fail(NSX_E_ARG, "x and y must not alias");
-    NSX_CUDA(cudaSetDevice(h->device));
+    require_device(h);
     matvec_device(h, x, y, precision, (cudaStream_t)stream);
   });
 }
@@ -190,7 +201,7 @@ int nsx_matvec_noalloc(nsx_handle *h, const double *x, double *y, void *stream) 
 int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision) {
   return guarded([&] {
     if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
-    NSX_CUDA(cudaSetDevice(h->device));
+    require_device(h);
     size_t bytes = sizeof(double) * h->no_state;
     NSX_CUDA(cudaMemcpy(h->d.xin, x, bytes, cudaMemcpyHostToDevice));
     matvec_device(h, h->d.xin, h->d.xout, precision, 0);
@@ -201,7 +212,7 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs, nsx_report *report) {
   return guarded([&] {
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
-    NSX_CUDA(cudaSetDevice(h->device));
+    require_device(h);
     solve(h, params, evals, evecs, report);
   });
 }
@@ -222,7 +233,7 @@ int nsx_stats_reset(nsx_handle *h, int32_t timing) {
 int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
   return guarded([&] {
     if (!h || !out) fail(NSX_E_ARG, "null argument");
-    NSX_CUDA(cudaSetDevice(h->device));
+    if (h->device >= 0) NSX_CUDA(cudaSetDevice(h->device));
     flush_stage_events(h);
     out->launches = h->launches;
     out->matvecs = h->matvecs;
@@ -238,7 +249,7 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
 
 void nsx_destroy(nsx_handle *h) {
   if (!h) return;
-  cudaSetDevice(h->device);
+  if (h->device >= 0) cudaSetDevice(h->device);
   release(h);
   delete h;
 }

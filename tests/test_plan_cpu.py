@@ -1,0 +1,90 @@
+"""Plan-only handles (nsx_create / nsx_load_files with device < 0): the host logic of the
+library without a GPU -- block list, offsets and parity mask against the generator (in memory
+and through the C++ file reader), interaction updates, and the reference's output files read
+back as NuVec reads them."""
+import os
+import numpy as np
+import pytest
+
+from conftest import make_problem, write_files
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    from nushellx_b200.build import build
+    build()
+
+
+@pytest.mark.parametrize("name", ["sd_2p2n_2", "fp_4p4n_0"])
+def test_plan_matches_the_generator(name, files_dir):
+    from nushellx_b200.nsx import Solver
+    P = make_problem(name)
+    for S in (Solver.from_problem(P, device=-1),
+              Solver.from_files(write_files(P, os.path.join(files_dir, "plan_" + name), name), device=-1)):
+        assert S.dim == P.no_state
+        assert [tuple(b[:2]) for b in S.blocks] == [tuple(b) for b in P.blocks]
+        assert [tuple(b[2:]) for b in S.blocks] == [tuple(d) for d in P.dims]
+        assert np.array_equal(S.offsets, P.offsets)
+        assert np.array_equal(S.lcoef, P.lcoef)
+        assert S.flops > 0
+        S.close()
+
+
+def test_plan_only_handle_refuses_device_work():
+    from nushellx_b200.nsx import Solver, NsxError, NSX_FP64
+    S = Solver.from_problem(make_problem("sd_2p2n_0"), device=-1)
+    with pytest.raises(NsxError, match="plan only"):
+        S.matvec_host(np.ones(S.dim), NSX_FP64)
+    with pytest.raises(NsxError, match="plan only"):
+        S.solve(nev=2)
+    with pytest.raises(NsxError, match="plan only"):
+        Solver.batch_solve([S], nev=2)
+    S.stats_reset()
+    assert S.stats()["launches"] == 0
+    S.close()
+
+
+def test_interaction_update_on_a_plan_only_handle():
+    from nushellx_b200.nsx import Solver, NsxError
+    from nushellx_b200.gen.variants import InteractionFamily
+    P = make_problem("sd_2p2n_2")
+    fam = InteractionFamily(P)
+    S = Solver.from_problem(P, device=-1)
+    S.set_interaction(*fam.arrays(np.full(8, 0.1)))
+    op, a, b = fam.arrays(np.zeros(8))
+    with pytest.raises(NsxError, match="op_vals holds"):
+        S.set_interaction(op[:-1], a, b)
+    with pytest.raises(NsxError, match="segment value counts"):
+        S.set_interaction(op, a[:-1], b)
+    bad = op.copy()
+    bad[0] = np.nan
+    with pytest.raises(NsxError, match="not finite"):
+        S.set_interaction(bad, a, b)
+    S.close()
+
+
+@pytest.mark.parametrize("name", ["sd_2p2n_0", "fp_4p4n_0"])
+def test_output_files_round_trip_without_a_gpu(name, tmp_path):
+    from nushellx_b200.nsx import Solver
+    from test_outputs import read_outputs, read_records
+    import struct
+    P = make_problem(name)
+    S = Solver.from_problem(P, device=-1)
+    nev = 5
+    rng = np.random.default_rng(3)
+    Q, _ = np.linalg.qr(rng.standard_normal((S.dim, nev)) * S.lcoef[:, None])
+    vecs = Q.T.copy()
+    ev = np.sort(rng.uniform(-5, 5, nev))
+    prefix = str(tmp_path / "out")
+    S.write_results(prefix, ev, vecs, 123, "synthetic", 0)
+    w, psi, lv, par = read_outputs(prefix, S, nev)
+    assert np.allclose(w, ev, rtol=1e-6, atol=1e-6)
+    for i in range(nev):
+        s = np.sign(psi[i] @ vecs[i])
+        assert np.abs(s * psi[i] - vecs[i]).max() <= 1e-6 * np.abs(vecs[i]).max()
+    assert np.allclose(lv, ev, atol=6e-4) and set(par) == {"+"}
+    recs = read_records(prefix + ".xvc")
+    assert struct.unpack("<ii", recs[0]) == (S.dim, nev) and len(recs) == nev + 1
+    r2 = struct.unpack("<iifiiiiiiii", read_records(prefix + ".abz")[1])
+    assert r2[0] == 123
+    S.close()
