@@ -68,9 +68,12 @@ def dist_init(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:   # host-only ranks (the reference arm, tests): gloo
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -85,7 +88,8 @@ def max_over_ranks(v, world):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -193,7 +197,8 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC, "nev": NEV, "parallelism": "host cores (OpenMP)"},
+        "config": {"workload": WORKLOAD_DESC if args.workload == WORKLOAD else args.workload, "nev": NEV,
+                   "parallelism": "host cores (OpenMP)"},
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"C/OpenMP restatement of NuLnz (the Fortran reference has no compiler here): "
                                    f"2 pre-iterations + 6 Lanczos steps per step ({sample_s / max(args.steps, 1):.1f} s "
