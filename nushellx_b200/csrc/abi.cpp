@@ -25,7 +25,6 @@ int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 // Device calls on a handle: a plan-only handle (created with device < 0) has no device data.
 static void require_device(const nsx_handle *h) {
   if (h->device < 0) fail(NSX_E_ARG, "the handle was created without a device (plan only)");
-  NSX_CUDA(cudaSetDevice(h->device));
 }
 
 template <typename F>
@@ -73,7 +72,7 @@ int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
       build_plan(h, prob);
       return;
     }
-    NSX_CUDA(cudaSetDevice(device));
+    DeviceGuard dg(device);
     build_plan(h, prob);
     upload(h);
   });
@@ -103,6 +102,7 @@ int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const
   return guarded([&] {
     if (!h) fail(NSX_E_ARG, "null handle");
     set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals);
+    DeviceGuard dg(h->device);
     if (h->device >= 0) upload_interaction(h);
   });
 }
@@ -190,6 +190,7 @@ int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, voi
     if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
     if (x == y) fail(NSX_E_ARG, "x and y must not alias");
     require_device(h);
+    DeviceGuard dg(h->device);
     matvec_device(h, x, y, precision, (cudaStream_t)stream);
   });
 }
@@ -202,6 +203,7 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
   return guarded([&] {
     if (!h || !x || !y) fail(NSX_E_ARG, "null argument");
     require_device(h);
+    DeviceGuard dg(h->device);
     size_t bytes = sizeof(double) * h->no_state;
     NSX_CUDA(cudaMemcpy(h->d.xin, x, bytes, cudaMemcpyHostToDevice));
     matvec_device(h, h->d.xin, h->d.xout, precision, 0);
@@ -213,6 +215,7 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
   return guarded([&] {
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
     require_device(h);
+    DeviceGuard dg(h->device);
     solve(h, params, evals, evecs, report);
   });
 }
@@ -220,6 +223,7 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
 int nsx_stats_reset(nsx_handle *h, int32_t timing) {
   return guarded([&] {
     if (!h) fail(NSX_E_ARG, "null handle");
+    DeviceGuard dg(h->device);
     flush_stage_events(h);
     h->launches = h->matvecs = 0;
     for (int i = 0; i < NSX_STAGES; ++i) {
@@ -233,7 +237,7 @@ int nsx_stats_reset(nsx_handle *h, int32_t timing) {
 int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
   return guarded([&] {
     if (!h || !out) fail(NSX_E_ARG, "null argument");
-    if (h->device >= 0) NSX_CUDA(cudaSetDevice(h->device));
+    DeviceGuard dg(h->device);
     flush_stage_events(h);
     out->launches = h->launches;
     out->matvecs = h->matvecs;
@@ -249,8 +253,12 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
 
 void nsx_destroy(nsx_handle *h) {
   if (!h) return;
-  if (h->device >= 0) cudaSetDevice(h->device);
-  release(h);
+  try {
+    DeviceGuard dg(h->device);
+    release(h);
+  } catch (...) {
+    release(h);   // the device could not be made current: free what the current context can
+  }
   delete h;
 }
 

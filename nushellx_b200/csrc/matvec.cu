@@ -606,7 +606,6 @@ static void dev_refill(T *p, const std::vector<double> &v) {
 // device buffers the handle already holds, in every precision that has been set up.  The
 // copies are synchronous, so products issued afterwards on any stream see the new values.
 void upload_interaction(nsx_handle *h) {
-  NSX_CUDA(cudaSetDevice(h->device));
   NSX_CUDA(cudaDeviceSynchronize());  // no product of the old interaction may still read them
   auto &d = h->d;
   dev_refill<double>(d.w, h->weights);
@@ -628,7 +627,6 @@ cudaStream_t solve_stream(nsx_handle *h) {
 }
 
 void upload(nsx_handle *h) {
-  NSX_CUDA(cudaSetDevice(h->device));
   if (h->max_anl > KA_MAXNL) fail(NSX_E_ARG, "proton partition with more than 64 J-states: not supported by k_a");
   auto &d = h->d;
   d.rhoB = dev_copy<double>(h->yrho);

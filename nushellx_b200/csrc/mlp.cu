@@ -37,6 +37,19 @@ void mcheck(cudaError_t e, const char *what) {
 }
 #define MCUDA(x) mcheck((x), #x)
 
+// Makes the network's device current for one entry point and restores the caller's device.
+struct MDevice {
+  int prev = -1;
+  explicit MDevice(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) MCUDA(cudaSetDevice(device));
+  }
+  ~MDevice() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 template <typename F>
 int mguard(F &&f) {
   try {
@@ -284,7 +297,7 @@ int nsx_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64_t seed, in
     if (n_in <= 0 || width <= 0 || n_out <= 0 || n_in > 4096 || width > 4096 || n_out > 4096)
       throw Err{NSX_E_ARG, "layer sizes out of range (1 .. 4096)"};
     q->device = device;
-    MCUDA(cudaSetDevice(device));
+    MDevice dg(device);
     q->n_in = n_in;
     q->width = width;
     q->n_out = n_out;
@@ -334,7 +347,7 @@ int nsx_mlp_set_params(nsx_mlp *q, const float *params, int64_t n) {
   return mguard([&] {
     check_handle(q);
     if (!params || n != q->np) throw Err{NSX_E_ARG, "parameter count mismatch"};
-    MCUDA(cudaSetDevice(q->device));
+    MDevice dg(q->device);
     MCUDA(cudaMemcpy(q->p, params, sizeof(float) * n, cudaMemcpyHostToDevice));
     MCUDA(cudaMemset(q->m, 0, sizeof(float) * n));
     MCUDA(cudaMemset(q->v, 0, sizeof(float) * n));
@@ -346,7 +359,7 @@ int nsx_mlp_get_params(const nsx_mlp *q, float *params, int64_t n) {
   return mguard([&] {
     check_handle(q);
     if (!params || n != q->np) throw Err{NSX_E_ARG, "parameter count mismatch"};
-    MCUDA(cudaSetDevice(q->device));
+    MDevice dg(q->device);
     MCUDA(cudaMemcpy(params, q->p, sizeof(float) * n, cudaMemcpyDeviceToHost));
   });
 }
@@ -356,7 +369,7 @@ int nsx_mlp_forward(nsx_mlp *q, const float *x, int32_t batch, float *y) {
     check_handle(q);
     check_batch(batch);
     if (!x || !y) throw Err{NSX_E_ARG, "null argument"};
-    MCUDA(cudaSetDevice(q->device));
+    MDevice dg(q->device);
     upload_batch(q, x, nullptr, batch);
     q->forward(batch);
     MCUDA(cudaMemcpy(y, q->y, sizeof(float) * (size_t)batch * q->n_out, cudaMemcpyDeviceToHost));
@@ -368,7 +381,7 @@ int nsx_mlp_gradients(nsx_mlp *q, const float *x, const float *t, int32_t batch,
     check_handle(q);
     check_batch(batch);
     if (!x || !t) throw Err{NSX_E_ARG, "null argument"};
-    MCUDA(cudaSetDevice(q->device));
+    MDevice dg(q->device);
     upload_batch(q, x, t, batch);
     q->forward(batch);
     q->backward(batch);
@@ -382,7 +395,7 @@ int nsx_mlp_train(nsx_mlp *q, const float *x, const float *t, int32_t batch, int
     check_handle(q);
     check_batch(batch);
     if (!x || !t || steps < 0) throw Err{NSX_E_ARG, "bad argument"};
-    MCUDA(cudaSetDevice(q->device));
+    MDevice dg(q->device);
     upload_batch(q, x, t, batch);
     for (int s = 0; s < steps; ++s) {
       q->forward(batch);
@@ -398,10 +411,13 @@ int nsx_mlp_train(nsx_mlp *q, const float *x, const float *t, int32_t batch, int
 
 void nsx_mlp_destroy(nsx_mlp *q) {
   if (!q) return;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   cudaSetDevice(q->device);
   q->free_batch();
   for (void *ptr : {(void *)q->p, (void *)q->g, (void *)q->m, (void *)q->v, (void *)q->loss})
     if (ptr) cudaFree(ptr);
+  if (prev >= 0 && prev != q->device) cudaSetDevice(prev);
   delete q;
 }
 

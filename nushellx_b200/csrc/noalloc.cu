@@ -11,39 +11,30 @@
 // * The array holds NOALLOC_Y_MAX FP64 elements (64 MiB); a problem whose
 //   intermediates (Y and the stacked Zbar) need more is rejected with NSX_E_ARG
 //   and a message.
-// * The first call on a device looks up the array's device address (this
-//   loads the library's module on that device if it is not loaded yet); make
-//   that first call before any stream capture.  Every GPU that loads the
+// * Every call looks up the array's device address on the handle's device
+//   (the first call on a device loads the library's module there if it is not
+//   loaded yet); make that first call before any stream capture.  Every GPU that loads the
 //   library holds the array until the process exits.
 // * All calls share the one array and it keeps the last call's contents; the
 //   product writes every scratch element it later reads, so the previous
 //   call's contents do not matter and nothing is cleared.  Calls that overlap
 //   on the GPU (different streams, or different handles on the same device,
 //   without ordering) race on the array.
-#include <mutex>
 #include "nsx_internal.h"
 
 namespace nsx {
 
 constexpr int64_t NOALLOC_Y_MAX = int64_t(8) << 20;  // FP64 elements (64 MiB)
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) double g_noalloc_y[NOALLOC_Y_MAX];
 
-static std::mutex g_noalloc_mu;
-static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
-
-// Device address of g_noalloc_y on the current device (looked up once per device).
-static double *noalloc_scratch(int device) {
-  if (device < 0 || device >= NOALLOC_MAX_DEVICES) fail(NSX_E_ARG, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_y);
-    if (e != cudaSuccess) fail(NSX_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_y): ") + cudaGetErrorString(e));
-    g_noalloc_ptr[device] = static_cast<double *>(p);
-  }
-  return g_noalloc_ptr[device];
+// Device address of g_noalloc_y on the current device.  Looked up on every call (cheap once
+// the module is loaded on the device), so a cached address can never outlive a context reset.
+static double *noalloc_scratch() {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_y);
+  if (e != cudaSuccess) fail(NSX_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_y): ") + cudaGetErrorString(e));
+  return static_cast<double *>(p);
 }
 
 int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
@@ -57,8 +48,12 @@ int nsx::noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream
   if (need > NOALLOC_Y_MAX)
     fail(NSX_E_ARG, "problem needs " + std::to_string(need) + " FP64 scratch elements; the fixed array of "
                         "nsx_matvec_noalloc holds " + std::to_string(NOALLOC_Y_MAX) + " (use nsx_matvec)");
-  NSX_CUDA(cudaSetDevice(h->device));
-  double *Y = noalloc_scratch(h->device);
+  if (h->device < 0) fail(NSX_E_CUDA, "the handle was created without a device (plan only)");
+  DeviceGuard dg(h->device);
+  double *Y = noalloc_scratch();
+  // k_a copies Zbar rows with 16-byte asynchronous copies: Zbar must start 16-byte aligned
+  if ((reinterpret_cast<uintptr_t>(Y + zbar_scratch_offset(h)) & 15) != 0)
+    fail(NSX_E_CUDA, "the Zbar part of the fixed scratch array is not 16-byte aligned");
   cudaStream_t s = (cudaStream_t)stream;
   // the array holds Y then Zbar; the Y stage writes every element of Y (zeros where no density
   // block reaches) and the mixing stage every element of Zbar, so nothing is cleared beforehand

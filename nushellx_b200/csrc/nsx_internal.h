@@ -18,6 +18,24 @@ struct Error {
 void check_cuda(cudaError_t e, const char *what);
 #define NSX_CUDA(x) ::nsx::check_cuda((x), #x)
 
+// Makes `device` current for the lifetime of the guard and then restores the caller's current
+// device, so that an entry point never leaves a multi-GPU host on another device than it chose.
+// device < 0 (plan-only handles) leaves the current device alone.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {
+    if (device < 0) return;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) check_cuda(cudaSetDevice(device), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 // One density sub-block: left partition pl, right partition pr, value offset.
 struct RhoBlk {
   int pl, pr;

@@ -102,3 +102,28 @@ def test_matvec_device_pointers_and_bad_arguments():
         S.matvec(x.data_ptr(), x.data_ptr(), NSX_FP64)      # aliasing
     with pytest.raises(NsxError):
         S.matvec(x.data_ptr(), y.data_ptr(), 7)             # unknown precision
+
+
+def test_matvec_benchmark_workload_matches_oracle(files_dir):
+    """The benchmarked workload itself (fp 6p+6n, J=0+, dimension 1,777,116): H.v from the
+    reference-format files against the FP64 oracle on two random vectors.  It reaches the
+    paths the small cases do not: Y tiles of more than one row tile, proton slabs whose stacked
+    operand is longer than one pipeline pass, and mixing groups with more than 8 sources."""
+    from oracle.jscheme import Oracle
+    from nushellx_b200.nsx import Solver, NSX_FP64, NSX_FP32
+    name = "fp_6p6n_0"
+    P = make_problem(name)
+    man = write_files(P, os.path.join(files_dir, name), name)
+    O = Oracle(man)
+    S = Solver.from_files(man)
+    assert S.dim == O.dim == 1777116
+    assert np.array_equal(S.lcoef, O.lcoef)
+    rng = np.random.default_rng(2024)
+    for trial in range(2):
+        x = rng.standard_normal(S.dim)
+        y_ref = O.matvec(x)
+        y64 = S.matvec_host(x, NSX_FP64)
+        assert _rel(y64, y_ref) < FP64_TOL, _rel(y64, y_ref)
+        y32 = S.matvec_host(x, NSX_FP32)
+        assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
+    S.close()

@@ -68,3 +68,30 @@ def test_noalloc_rejects_problems_beyond_the_fixed_size():
     with pytest.raises(NsxError, match="scratch"):
         S.matvec_noalloc(x.data_ptr(), y.data_ptr())
     S.close()
+
+
+def test_noalloc_first_on_a_fresh_handle_allocates_nothing():
+    """No nsx_matvec before it on the handle (so nothing it allocated can be relied on), and the
+    device's free memory is the same before and after further calls.  The first call on a
+    device may load the library's module (and with it the fixed array), so the free-memory
+    check brackets the calls after it."""
+    import torch
+    from nushellx_b200.nsx import Solver, NSX_FP64
+    S = Solver.from_problem(make_problem("sd_2p2n_2"))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    xs = [torch.randn(S.dim, dtype=torch.float64, device="cuda", generator=g) for _ in range(3)]
+    ys = [torch.full_like(xs[0], float("nan")) for _ in range(3)]
+    S.matvec_noalloc(xs[0].data_ptr(), ys[0].data_ptr())
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for i in (1, 2):
+        S.matvec_noalloc(xs[i].data_ptr(), ys[i].data_ptr())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    for x, y in zip(xs, ys):
+        y_ref = torch.empty_like(x)
+        S.matvec(x.data_ptr(), y_ref.data_ptr(), NSX_FP64)
+        torch.cuda.synchronize()
+        assert _rel(y, y_ref) < TOL
+    S.close()
