@@ -487,6 +487,133 @@ double ref_lanczos(ref_handle *h, int npre, int nsteps, uint64_t seed, double *a
   return t2 - t1;
 }
 
+/* Number of eigenvalues below x of the symmetric tridiagonal matrix (diagonal a[0..n),
+ * off-diagonal b[1..n)), by the Sturm sequence of its LDL^T factorisation (Golub & Van Loan,
+ * Matrix Computations, section 8.4.1). */
+static int sturm_count(const double *a, const double *b, int n, double x) {
+  int cnt = 0;
+  double q = a[0] - x;
+  if (q < 0) ++cnt;
+  for (int i = 1; i < n; ++i) {
+    if (q == 0.0) q = 1e-300;
+    q = a[i] - x - b[i] * b[i] / q;
+    if (q < 0) ++cnt;
+  }
+  return cnt;
+}
+/* The k lowest eigenvalues of that matrix by bisection (out[0..k) ascending). */
+static void tri_lowest(const double *a, const double *b, int n, int k, double *out) {
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < n; ++i) {
+    double r = (i > 0 ? fabs(b[i]) : 0.0) + (i + 1 < n ? fabs(b[i + 1]) : 0.0);
+    if (a[i] - r < lo) lo = a[i] - r;
+    if (a[i] + r > hi) hi = a[i] + r;
+  }
+  const double eps = 1e-13 * (fabs(lo) + fabs(hi) + 1.0);
+  for (int j = 0; j < k && j < n; ++j) {
+    double l = lo, u = hi;
+    while (u - l > eps) {
+      double m = 0.5 * (l + u);
+      if (sturm_count(a, b, n, m) > j) u = m; else l = m;
+    }
+    out[j] = 0.5 * (l + u);
+  }
+}
+
+/* A complete solve by the reference's standard Lanczos (NuLnz Lnz_OP, NuCoreX.f90:595-751):
+ * seeded start on the allowed entries, npre power pre-iterations, the three-term recurrence
+ * with classical Gram-Schmidt against every stored vector (vectors in RAM), breakdown restart
+ * below restart_limit, and its stopping rule: the first test after first_iter steps, then
+ * every inc_iter + 1 steps, until the lowest nlev + 1 Ritz values change by less than
+ * level_limit between tests, or noiter steps.  Writes the lowest nlev Ritz values and the
+ * step count; returns the wall seconds of the whole solve (pre-iterations included). */
+double ref_solve(ref_handle *h, int npre, int nlev, int first_iter, int inc_iter, int noiter, double level_limit,
+                 uint64_t seed, double *evals, int *iterations) {
+  const int64_t N = h->no_state;
+  float *V = malloc(sizeof(float) * N * (size_t)(noiter + 1));
+  memset(V, 0, sizeof(float) * N * (size_t)(noiter + 1));
+  float *L = malloc(sizeof(float) * N), *R = malloc(sizeof(float) * N), *Tv = malloc(sizeof(float) * N);
+  double *al = calloc((size_t)noiter + 2, sizeof(double)), *be = calloc((size_t)noiter + 2, sizeof(double));
+  double *prev = calloc((size_t)nlev + 2, sizeof(double)), *cur = calloc((size_t)nlev + 2, sizeof(double));
+  int64_t nallowed = 0;
+  for (int64_t i = 0; i < N; ++i) nallowed += h->lcoef[i] ? 1 : 0;
+  uint64_t z = seed ? seed : 5;
+  for (int64_t i = 0; i < N; ++i) {
+    z = z * 6364136223846793005ull + 1442695040888963407ull;
+    float x = (float)((z >> 11) * (1.0 / 9007199254740992.0));
+    L[i] = h->lcoef[i] ? 0.5f - x : 0.0f;
+  }
+  double t0 = omp_get_wtime();
+  float ovl = (float)(1.0 / sqrt(dot44(L, L, N)));
+  for (int64_t i = 0; i < N; ++i) R[i] = ovl * L[i];
+  for (int it = 0; it < npre; ++it) {
+    ref_matvec(h, R, L);
+    ovl = (float)(1.0 / sqrt(dot44(L, L, N)));
+    for (int64_t i = 0; i < N; ++i) R[i] = ovl * L[i];
+  }
+  memcpy(V, R, sizeof(float) * N);
+  float b = 0;
+  int it = 0, next_test = first_iter, done = 0;
+  const int nk = nlev + 1;
+  for (; it < noiter && !done; ++it) {
+    ref_matvec(h, R, L);
+    if (it) {
+#pragma omp parallel for
+      for (int64_t i = 0; i < N; ++i) L[i] -= b * Tv[i];
+    }
+    memcpy(Tv, R, sizeof(float) * N);
+    float a = (float)dot44(R, L, N);
+    al[it] = a;
+    if (it + 1 >= nallowed) { ++it; break; }   /* Krylov space complete */
+#pragma omp parallel for
+    for (int64_t i = 0; i < N; ++i) L[i] -= a * R[i];
+    memcpy(R, L, sizeof(float) * N);
+    for (int j = 0; j <= it; ++j) {
+      const float *vj = V + (size_t)j * N;
+      double s = 0;
+#pragma omp parallel for reduction(+ : s)
+      for (int64_t i = 0; i < N; ++i) s += (double)R[i] * vj[i];
+      const float o = (float)s;
+#pragma omp parallel for
+      for (int64_t i = 0; i < N; ++i) L[i] -= o * vj[i];
+    }
+    double nb = sqrt(dot44(L, L, N));
+    if (nb > 1e-7) {
+      b = (float)nb;
+    } else {   /* breakdown: a random direction orthogonal to the stored vectors, zero coupling */
+      for (int64_t i = 0; i < N; ++i) {
+        z = z * 6364136223846793005ull + 1442695040888963407ull;
+        L[i] = h->lcoef[i] ? (float)(1000.0 * ((z >> 11) * (1.0 / 9007199254740992.0))) * L[i] : 0.0f;
+      }
+      for (int j = 0; j <= it; ++j) {
+        const float *vj = V + (size_t)j * N;
+        const float o = (float)dot44(L, vj, N);
+        for (int64_t i = 0; i < N; ++i) L[i] -= o * vj[i];
+      }
+      nb = sqrt(dot44(L, L, N));
+      if (nb < 1e-7) { ++it; break; }
+      b = 0.0f;
+    }
+    be[it + 1] = b;
+    const float inv = (float)(1.0 / nb);
+    for (int64_t i = 0; i < N; ++i) R[i] = inv * L[i];
+    memcpy(V + (size_t)(it + 1) * N, R, sizeof(float) * N);
+    if (it + 1 == next_test) {
+      tri_lowest(al, be, it + 1, nk, cur);
+      done = 1;
+      for (int j = 0; j < nk && j < it + 1; ++j)
+        if (fabs(cur[j] - prev[j]) > level_limit) done = 0;
+      memcpy(prev, cur, sizeof(double) * (size_t)nk);
+      next_test = it + 1 + inc_iter + 1;
+    }
+  }
+  double t1 = omp_get_wtime();
+  tri_lowest(al, be, it, nlev, evals);
+  *iterations = it;
+  free(V); free(L); free(R); free(Tv); free(al); free(be); free(prev); free(cur);
+  return t1 - t0;
+}
+
 void ref_destroy(ref_handle *h) {
   if (!h) return;
   /* process-lifetime baseline objects: release the large buffers */

@@ -25,6 +25,9 @@ def lib():
         L.ref_lanczos.restype = C.c_double
         L.ref_lanczos.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_solve.restype = C.c_double
+        L.ref_solve.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64,
+                                C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.ref_destroy.restype = None
         L.ref_destroy.argtypes = [C.c_void_p]
         _lib = L
@@ -34,9 +37,19 @@ def lib():
 class RefSolver:
     """The reference algorithm (FP32 storage, axpy order, OpenMP) on a generated problem."""
 
-    def __init__(self, P):
+    def __init__(self, P, variant=None):
+        """variant: optional (op_vals, a_seg_vals, b_seg_vals) of an interaction variant in the
+        order of P's operator keys and segments (InteractionFamily.arrays), used instead of
+        P's own interaction."""
         from nushellx_b200.nsx import build_problem_struct
         self._prob, self._keep = build_problem_struct(P)
+        if variant is not None:
+            op, av, bv = (np.ascontiguousarray(v, dtype=np.float64) for v in variant)
+            assert len(op) == self._prob.nop
+            self._keep.append((op, av, bv))
+            self._prob.op_vals = op.ctypes.data_as(C.POINTER(C.c_double))
+            self._prob.a.seg_vals = av.ctypes.data_as(C.POINTER(C.c_double))
+            self._prob.b.seg_vals = bv.ctypes.data_as(C.POINTER(C.c_double))
         self._h = lib().ref_create(C.byref(self._prob))
         self.dim = int(lib().ref_dim(self._h))
         self.threads = int(lib().ref_nthreads(self._h))
@@ -57,6 +70,16 @@ class RefSolver:
         t = lib().ref_lanczos(self._h, npre, nsteps, seed, a.ctypes.data_as(C.POINTER(C.c_double)),
                               b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pre), C.byref(cgs))
         return t, pre.value, cgs.value, a[:nsteps], b[:nsteps]
+
+    def solve(self, nlev=10, npre=2, first_iter=90, inc_iter=3, noiter=300, level_limit=5e-4, seed=5):
+        """A complete solve by the reference's standard Lanczos and its own stopping rule
+        (src/NuLnz/NuCoreX.f90:595-751; parameters from src/NuCommon/NuCommon.f90:101-124 and
+        src/NuCommonX/NuCommonX.f90:23-27).  Returns (lowest nlev Ritz values, steps, seconds)."""
+        ev = np.zeros(nlev)
+        it = C.c_int(0)
+        t = lib().ref_solve(self._h, npre, nlev, first_iter, inc_iter, noiter, level_limit, seed,
+                            ev.ctypes.data_as(C.POINTER(C.c_double)), C.byref(it))
+        return ev, it.value, t
 
     def close(self):
         if self._h:
