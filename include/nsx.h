@@ -131,6 +131,27 @@ typedef struct nsx_files {
 
 int nsx_load_files(const nsx_files *files, int device, nsx_handle **out);
 
+/* The compressed pn interaction of NuTRLZ (src/NuTRLZ/NuCoreXZ.f90:1613-1887, read from the
+ * .dop file that src/NuDiop/NuDiop.f90 writes): for each (2lam, parity) the kept eigenpairs
+ * (e, u_e) of the multipole matrix V_lam(proton pair; neutron pair), one term per kept
+ * component of an eigenvector.  The handle's proton densities are folded into the combined
+ * operators sum_a e u_e(a) rho_a, the neutron densities into sum_b u_e(b) rho_b, and the pn
+ * product pairs the combined operators of the same e with the Racah weight alone (the
+ * problem's own op_keys / op_vals are not used; renorm is).  Without truncation this is the
+ * exact product; with it, the approximation NuTRLZ makes. */
+typedef struct nsx_dop {
+  int32_t nterms;            /* kept eigenvector components                          */
+  const int32_t *lam2;       /* [nterms] 2lam                                         */
+  const int32_t *parity;     /* [nterms] +1 / -1: parity of the orbit pairs           */
+  const int32_t *eig;        /* [nterms] eigenvector number within its (2lam, parity), 1.. */
+  const double *e;           /* [nterms] its eigenvalue (MeV)                          */
+  const uint8_t *shells;     /* [nterms][4]: proton shells s1 s3, neutron shells s2 s4 */
+  const double *u;           /* [nterms] the component u_e(s1 s3) = u_e(s2 s4)         */
+} nsx_dop;
+int nsx_create_z(const nsx_problem *prob, const nsx_dop *dop, int device, nsx_handle **out);
+/* The same from the file set of nsx_load_files plus the .dop file at dop_path. */
+int nsx_load_files_z(const nsx_files *files, const char *dop_path, int device, nsx_handle **out);
+
 /* Replace the interaction of a handle without re-planning: new pn multipole values
  * (op_vals, same count and order as nsx_problem.op_keys at creation, renorm applied as
  * then) and new like-particle segment values (same segments and order as the
@@ -215,6 +236,24 @@ typedef struct nsx_stats {
   double stage_bytes[NSX_STAGES];  /* algorithmic HBM bytes of one launch of each stage  */
   double stage_flops[NSX_STAGES];  /* algorithmic flops of one launch of each stage      */
 } nsx_stats;
+
+/* Shape of a handle's H.v plan (no counterpart in the reference): which kernel paths its
+ * products take and the sizes that select them.  For tests and profiling; works on plan-only
+ * handles. */
+typedef struct nsx_plan_info {
+  int64_t y_elems;            /* Y intermediate elements (k_y path)                           */
+  int64_t zbar_elems;         /* stacked operand elements, FP64 row-major layout              */
+  int64_t zbar_tc_elems;      /* stacked operand elements, FP32 tensor-core tile layout       */
+  int32_t y_row_tiles_max;    /* most 256-row tiles of one Y matrix (k_y)                     */
+  int32_t group_sources_max;  /* most sources (h, b) of one mixing group                      */
+  int32_t fused_fp32;         /* 1: the FP32 form forms Y inside the mixing stage (k_yz)      */
+  int32_t slab_rows_max;      /* longest stacked operand of an output slab                    */
+  int32_t slab_splits_max;    /* most K pieces of one FP64 k_a slab tile (atomic partial sums) */
+  int32_t slab_nl_max;        /* most rows of a proton partition (an output slab)             */
+  int64_t tc_tiles[4];        /* k_a_tc tiles with N = 16, 32, 48, 64                         */
+  int64_t tc_chunks_max;      /* most 32-row pipeline stages of one k_a_tc tile               */
+} nsx_plan_info;
+int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out);
 
 /* Reset the counters; enable (1) or disable (0) per-stage event timing. */
 int nsx_stats_reset(nsx_handle *h, int32_t timing);

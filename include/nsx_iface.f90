@@ -67,7 +67,38 @@ module nsx_iface
      real(c_double)     :: stage_ms(NSX_STAGES), stage_bytes(NSX_STAGES), stage_flops(NSX_STAGES)
   end type nsx_stats
 
+  type, bind(C) :: nsx_dop
+     integer(c_int32_t) :: nterms
+     type(c_ptr)        :: lam2, parity, eig, e, shells, u
+  end type nsx_dop
+
+  type, bind(C) :: nsx_plan_info
+     integer(c_int64_t) :: y_elems, zbar_elems, zbar_tc_elems
+     integer(c_int32_t) :: y_row_tiles_max, group_sources_max, fused_fp32
+     integer(c_int32_t) :: slab_rows_max, slab_splits_max, slab_nl_max
+     integer(c_int64_t) :: tc_tiles(4), tc_chunks_max
+  end type nsx_plan_info
+
   interface
+     integer(c_int) function nsx_create_z(prob, dop, device, out) bind(C, name="nsx_create_z")
+       import :: c_int, c_ptr, nsx_problem, nsx_dop
+       type(nsx_problem), intent(in) :: prob
+       type(nsx_dop), intent(in) :: dop
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_load_files_z(files, dop_path, device, out) bind(C, name="nsx_load_files_z")
+       import :: c_int, c_ptr, c_char, nsx_files
+       type(nsx_files), intent(in) :: files
+       character(kind=c_char), dimension(*), intent(in) :: dop_path   ! NUL-terminated
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_get_plan_info(h, info) bind(C, name="nsx_get_plan_info")
+       import :: c_int, c_ptr, nsx_plan_info
+       type(c_ptr), value :: h
+       type(nsx_plan_info), intent(out) :: info
+     end function
      integer(c_int) function nsx_create(prob, device, out) bind(C, name="nsx_create")
        import :: c_int, c_ptr, nsx_problem
        type(nsx_problem), intent(in) :: prob

@@ -34,7 +34,7 @@ def _stale(target, deps):
 
 def build(verbose=False, force=False):
     srcs = sources()
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "nsx.h"))
     if not force and not _stale(LIB, srcs + headers):
         if _stale(CLI, [CLI_SRC, LIB]):

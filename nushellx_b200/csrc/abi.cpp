@@ -8,6 +8,7 @@
 #include <vector>
 #include <exception>
 #include <new>
+#include <map>
 #include "nsx_internal.h"
 
 namespace nsx {
@@ -20,6 +21,8 @@ void check_cuda(cudaError_t e, const char *what) {
 }
 void solve(nsx_handle *h, const nsx_params *P, double *evals, double *evecs, nsx_report *rep);
 std::shared_ptr<void> load_files(const nsx_files *f, nsx_problem *p);
+std::shared_ptr<void> compress_problem(const nsx_problem *p, const nsx_dop *d, nsx_problem *out);
+std::shared_ptr<DopArrays> read_dop(const std::string &path);
 int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 
 // Device calls on a handle: a plan-only handle (created with device < 0) has no device data.
@@ -95,6 +98,34 @@ int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
   });
   if (rc != NSX_OK) return rc;
   return nsx_create(&p, device, out);
+}
+
+int nsx_create_z(const nsx_problem *prob, const nsx_dop *dop, int device, nsx_handle **out) {
+  nsx_problem z;
+  std::memset(&z, 0, sizeof(z));
+  std::shared_ptr<void> store;
+  int rc = guarded([&] {
+    if (!prob || !dop || !out) fail(NSX_E_ARG, "null argument");
+    store = compress_problem(prob, dop, &z);
+  });
+  if (rc != NSX_OK) return rc;
+  return nsx_create(&z, device, out);
+}
+
+int nsx_load_files_z(const nsx_files *files, const char *dop_path, int device, nsx_handle **out) {
+  nsx_problem p, z;
+  std::memset(&p, 0, sizeof(p));
+  std::memset(&z, 0, sizeof(z));
+  std::shared_ptr<void> store, zstore;
+  int rc = guarded([&] {
+    if (!files || !dop_path || !out) fail(NSX_E_ARG, "null argument");
+    store = load_files(files, &p);
+    auto dop = read_dop(dop_path);
+    nsx_dop d = dop->view();
+    zstore = compress_problem(&p, &d, &z);
+  });
+  if (rc != NSX_OK) return rc;
+  return nsx_create(&z, device, out);
 }
 
 int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
@@ -208,6 +239,7 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
     NSX_CUDA(cudaMemcpy(h->d.xin, x, bytes, cudaMemcpyHostToDevice));
     matvec_device(h, h->d.xin, h->d.xout, precision, 0);
     NSX_CUDA(cudaMemcpy(y, h->d.xout, bytes, cudaMemcpyDeviceToHost));
+    check_device_error(h);
   });
 }
 
@@ -217,6 +249,7 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
     require_device(h);
     DeviceGuard dg(h->device);
     solve(h, params, evals, evecs, report);
+    check_device_error(h);
   });
 }
 
@@ -239,6 +272,7 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
     if (!h || !out) fail(NSX_E_ARG, "null argument");
     DeviceGuard dg(h->device);
     flush_stage_events(h);
+    if (h->device >= 0) check_device_error(h);
     out->launches = h->launches;
     out->matvecs = h->matvecs;
     // algorithmic figures for the precision of the last H.v
@@ -248,6 +282,28 @@ int nsx_get_stats(nsx_handle *h, nsx_stats *out) {
       out->stage_launches[i] = h->stage_launches[i];
       out->stage_ms[i] = h->stage_ms[i];
     }
+  });
+}
+
+int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out) {
+  return guarded([&] {
+    if (!h || !out) fail(NSX_E_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->y_elems = h->y_elems;
+    out->zbar_elems = h->z_elems;
+    out->zbar_tc_elems = h->z32_elems;
+    for (const auto &g : h->ygroups)
+      out->y_row_tiles_max = std::max(out->y_row_tiles_max, (g.m + KY_TILE_ROWS - 1) / KY_TILE_ROWS);
+    out->group_sources_max = h->max_zns;
+    out->fused_fp32 = h->max_zns <= 16 ? 1 : 0;
+    std::map<std::pair<int64_t, int32_t>, int> pieces;   // (slab out offset, col0) -> K pieces
+    for (const auto &t : h->atiles) {
+      out->slab_rows_max = std::max(out->slab_rows_max, t.k_end);
+      out->slab_nl_max = std::max(out->slab_nl_max, t.nl);
+      out->slab_splits_max = std::max(out->slab_splits_max, ++pieces[{t.out, t.col0}]);
+    }
+    for (int c = 0; c < 4; ++c) out->tc_tiles[c] = h->atc_off[c + 1] - h->atc_off[c];
+    for (const auto &t : h->atiles_tc) out->tc_chunks_max = std::max<int64_t>(out->tc_chunks_max, (t.kgroups + 3) / 4);
   });
 }
 

@@ -101,6 +101,131 @@ __global__ void __launch_bounds__(256) k_sub(const double *__restrict__ V, int64
     w[i] = s;
   }
 }
+// ---- classical Gram-Schmidt with a second pass (CGS2) in three passes over the basis ----
+// Pass 1 (k_cg_dot):    h  = V^T w                         (V and w read once)
+// Pass 2 (k_cg_subdot): w -= V h, then h2 = V^T w          (V read once: each 64-row slice of
+//                        the basis is staged in shared memory and used for both products)
+// Pass 3 (k_cg_subnrm): w -= V h2, ||w||^2                 (V read once)
+// Per-CTA partial sums go to partial[cta][CG_MAXJ] and are added in a fixed order by
+// k_cg_reduce (deterministic).
+constexpr int CG_MAXJ = 128;   // basis vectors per pass (the window is capped below it)
+constexpr int CG_ROWS = 64;    // rows per staged slice of k_cg_subdot
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(256) k_cg_dot(const double *__restrict__ V, int64_t ldv, int cnt,
+                                                const double *__restrict__ w, int64_t n, double *__restrict__ partial) {
+  __shared__ double acc[8][CG_MAXJ];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < 8 * CG_MAXJ; e += 256) (&acc[0][0])[e] = 0.0;
+  __syncthreads();
+  for (int64_t base = (int64_t)blockIdx.x * 1024; base < n; base += (int64_t)gridDim.x * 1024) {
+    double wv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t r = base + tid + 256 * k;
+      wv[k] = r < n ? w[r] : 0.0;
+    }
+    for (int j = 0; j < cnt; ++j) {
+      const double *vj = V + (int64_t)j * ldv;
+      double sj = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int64_t r = base + tid + 256 * k;
+        if (r < n) sj = fma(vj[r], wv[k], sj);
+      }
+      sj = warp_sum(sj);
+      if (lane == 0) acc[warp][j] += sj;
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < cnt; j += 256) {
+    double v = 0.0;
+    for (int q = 0; q < 8; ++q) v += acc[q][j];
+    partial[(int64_t)blockIdx.x * CG_MAXJ + j] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_cg_subdot(const double *__restrict__ V, int64_t ldv, int cnt,
+                                                   const double *__restrict__ h, double *__restrict__ w, int64_t n,
+                                                   double *__restrict__ partial) {
+  extern __shared__ double cg_sm[];
+  double *Vs = cg_sm;                              // [cnt][CG_ROWS + 1]
+  double *hs = Vs + (size_t)cnt * (CG_ROWS + 1);   // [cnt]
+  double *ws = hs + CG_MAXJ;                       // [CG_ROWS]
+  const int tid = threadIdx.x;
+  for (int j = tid; j < cnt; j += 256) hs[j] = h[j];
+  double accj = 0.0;                               // thread j < cnt: the partial of h2[j]
+  for (int64_t base = (int64_t)blockIdx.x * CG_ROWS; base < n; base += (int64_t)gridDim.x * CG_ROWS) {
+    const int rows = (int)(n - base < CG_ROWS ? n - base : CG_ROWS);
+    __syncthreads();
+    for (int e = tid; e < cnt * CG_ROWS; e += 256) {
+      const int j = e / CG_ROWS, r = e - j * CG_ROWS;
+      Vs[j * (CG_ROWS + 1) + r] = r < rows ? V[(int64_t)j * ldv + base + r] : 0.0;
+    }
+    __syncthreads();
+    {  // w -= V h for the slice: 4 threads per row
+      const int row = tid >> 2, q = tid & 3;
+      double sv = 0.0;
+      for (int j = q; j < cnt; j += 4) sv = fma(Vs[j * (CG_ROWS + 1) + row], hs[j], sv);
+      sv += __shfl_xor_sync(0xffffffffu, sv, 1);
+      sv += __shfl_xor_sync(0xffffffffu, sv, 2);
+      if (q == 0) {
+        const double w1 = row < rows ? w[base + row] - sv : 0.0;
+        ws[row] = w1;
+        if (row < rows) w[base + row] = w1;
+      }
+    }
+    __syncthreads();
+    if (tid < cnt) {
+      const double *vr = Vs + tid * (CG_ROWS + 1);
+#pragma unroll 8
+      for (int r = 0; r < CG_ROWS; ++r) accj = fma(vr[r], ws[r], accj);
+    }
+  }
+  if (tid < cnt) partial[(int64_t)blockIdx.x * CG_MAXJ + tid] = accj;
+}
+
+__global__ void __launch_bounds__(256) k_cg_subnrm(const double *__restrict__ V, int64_t ldv, int cnt,
+                                                   const double *__restrict__ h, double *__restrict__ w, int64_t n,
+                                                   double *__restrict__ partial) {
+  __shared__ double hs[CG_MAXJ];
+  __shared__ double red[8];
+  const int tid = threadIdx.x;
+  for (int j = tid; j < cnt; j += 256) hs[j] = h[j];
+  __syncthreads();
+  double nrm = 0.0;
+  for (int64_t r = (int64_t)blockIdx.x * 256 + tid; r < n; r += (int64_t)gridDim.x * 256) {
+    double sv = w[r];
+    for (int j = 0; j < cnt; ++j) sv = fma(-hs[j], V[(int64_t)j * ldv + r], sv);
+    w[r] = sv;
+    nrm = fma(sv, sv, nrm);
+  }
+  nrm = warp_sum(nrm);
+  if ((tid & 31) == 0) red[tid >> 5] = nrm;
+  __syncthreads();
+  if (tid == 0) {
+    double v = 0.0;
+    for (int q = 0; q < 8; ++q) v += red[q];
+    partial[(int64_t)blockIdx.x * CG_MAXJ] = v;
+  }
+}
+
+// out[j] = sum_cta partial[cta][j], j < cnt: one warp per j, fixed order
+__global__ void __launch_bounds__(256) k_cg_reduce(const double *__restrict__ partial, int nparts, int cnt,
+                                                   double *__restrict__ out) {
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (j >= cnt) return;
+  double v = 0.0;
+  for (int p = lane; p < nparts; p += 32) v += partial[(int64_t)p * CG_MAXJ + j];
+  v = warp_sum(v);
+  if (lane == 0) out[j] = v;
+}
+
 // v = w / sqrt(nrm2[0]) (zero if nrm2 == 0)
 __global__ void k_scale(const double *__restrict__ w, double *__restrict__ v, const double *__restrict__ nrm2,
                         int64_t n) {
@@ -242,17 +367,85 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
 }
 
 // ---------------------------------------------------------------------------
+// Device workspace of the solver, kept by the handle between solves (allocated by the first
+// solve and grown when a later one needs more), so that a solve allocates nothing once the
+// handle has solved a problem of its size: the basis V, the residual w, the rotation buffer,
+// the refinement's H Y, the reduction partials and the small matrices.
 struct Workspace {
-  double *V = nullptr, *w = nullptr, *tmp = nullptr, *partial = nullptr, *h = nullptr, *h2 = nullptr;
+  int64_t n = 0;
+  int vcap = 0, tcap = 0, mcap = 0, hycap = 0;
+  double *V = nullptr, *w = nullptr, *tmp = nullptr, *HY = nullptr, *partial = nullptr, *h = nullptr,
+         *h2 = nullptr;
   double *T = nullptr, *ev = nullptr, *S = nullptr;
   int *status = nullptr;
   uint8_t *mask = nullptr;
-  ~Workspace() {
-    void *p[] = {V, w, tmp, partial, h, h2, T, ev, S, status, mask};
+  void free_all() {
+    void *p[] = {V, w, tmp, HY, partial, h, h2, T, ev, S, status, mask};
     for (void *q : p)
       if (q) cudaFree(q);
+    *this = Workspace();
   }
 };
+
+void release_lanczos(nsx_handle *h) {
+  if (!h->lws) return;
+  Workspace *ws = static_cast<Workspace *>(h->lws);
+  ws->free_all();
+  delete ws;
+  h->lws = nullptr;
+}
+
+// The handle's workspace with room for a window of m, keep kept vectors and nev pairs.
+static Workspace &workspace(nsx_handle *h, int m, int keep, int nev, cudaStream_t s) {
+  if (!h->lws) h->lws = new Workspace();
+  Workspace &ws = *static_cast<Workspace *>(h->lws);
+  const int64_t n = h->no_state;
+  const int vneed = std::max(m + 1, 2 * nev), tneed = std::max(keep, nev);
+  if (ws.n == n && ws.vcap >= vneed && ws.tcap >= tneed && ws.mcap >= m && ws.hycap >= nev) return ws;
+  NSX_CUDA(cudaStreamSynchronize(s));
+  ws.free_all();
+  ws.n = n;
+  ws.vcap = vneed;
+  ws.tcap = tneed;
+  ws.mcap = m;
+  ws.hycap = nev;
+  NSX_CUDA(cudaMalloc(&ws.V, sizeof(double) * n * vneed));
+  NSX_CUDA(cudaMalloc(&ws.w, sizeof(double) * n));
+  NSX_CUDA(cudaMalloc(&ws.tmp, sizeof(double) * n * tneed));
+  NSX_CUDA(cudaMalloc(&ws.HY, sizeof(double) * n * nev));
+  NSX_CUDA(cudaMalloc(&ws.partial, sizeof(double) * RED_CTAS * std::max(JT, CG_MAXJ)));
+  NSX_CUDA(cudaMalloc(&ws.h, sizeof(double) * (m + 8)));
+  NSX_CUDA(cudaMalloc(&ws.h2, sizeof(double) * (m + 8)));
+  NSX_CUDA(cudaMalloc(&ws.T, sizeof(double) * m * m));
+  NSX_CUDA(cudaMalloc(&ws.ev, sizeof(double) * m));
+  NSX_CUDA(cudaMalloc(&ws.S, sizeof(double) * m * m));
+  NSX_CUDA(cudaMalloc(&ws.status, sizeof(int)));
+  NSX_CUDA(cudaMalloc(&ws.mask, n));
+  NSX_CUDA(cudaMemcpyAsync(ws.mask, h->lcoef.data(), n, cudaMemcpyHostToDevice, s));
+  NSX_CUDA(cudaStreamSynchronize(s));   // the mask copy from pageable memory has landed
+  return ws;
+}
+
+// CGS2 of w against the first cnt basis vectors: h = V^T w, w -= V h, h2 = V^T w, w -= V h2,
+// nrm2 = ||w||^2 (three passes over V, six launches).
+static void cgs2(Workspace &ws, int cnt, double *h, double *h2, double *nrm2, cudaStream_t s) {
+  const int64_t n = ws.n;
+  const double *V = ws.V;
+  count_launch();
+  k_cg_dot<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, ws.w, n, ws.partial);
+  count_launch();
+  k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h);
+  const size_t smem = sizeof(double) * ((size_t)cnt * (CG_ROWS + 1) + CG_MAXJ + CG_ROWS);
+  count_launch();
+  k_cg_subdot<<<RED_CTAS, 256, smem, s>>>(V, n, cnt, h, ws.w, n, ws.partial);
+  count_launch();
+  k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h2);
+  count_launch();
+  k_cg_subnrm<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, h2, ws.w, n, ws.partial);
+  count_launch();
+  k_cg_reduce<<<1, 256, 0, s>>>(ws.partial, RED_CTAS, 1, nrm2);
+  NSX_CUDA(cudaGetLastError());
+}
 
 static unsigned grid_for(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, RED_CTAS); }
 
@@ -292,6 +485,8 @@ static void ensure_kernel_attributes(int device) {
   if (done.count(device)) return;
   NSX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JACOBI_SMEM_MAX));
   NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROTATE_SMEM_MAX));
+  NSX_CUDA(cudaFuncSetAttribute(k_cg_subdot, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(double) * ((size_t)CG_MAXJ * (CG_ROWS + 1) + CG_MAXJ + CG_ROWS))));
   done.insert(device);
 }
 
@@ -387,20 +582,8 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     ~CounterScope() { g_launches = nullptr; }
   } counter_scope(&h->launches);
 
-  Workspace ws;
-  // basis (m+1 vectors); the FP64 refinement reuses it for 2*nev rotated vectors
-  NSX_CUDA(cudaMalloc(&ws.V, sizeof(double) * n * std::max(m + 1, 2 * nev)));
-  NSX_CUDA(cudaMalloc(&ws.w, sizeof(double) * n));
-  NSX_CUDA(cudaMalloc(&ws.tmp, sizeof(double) * n * std::max(keep, nev)));
-  NSX_CUDA(cudaMalloc(&ws.partial, sizeof(double) * RED_CTAS * JT));
-  NSX_CUDA(cudaMalloc(&ws.h, sizeof(double) * (m + 8)));
-  NSX_CUDA(cudaMalloc(&ws.h2, sizeof(double) * (m + 8)));
-  NSX_CUDA(cudaMalloc(&ws.T, sizeof(double) * m * m));
-  NSX_CUDA(cudaMalloc(&ws.ev, sizeof(double) * m));
-  NSX_CUDA(cudaMalloc(&ws.S, sizeof(double) * m * m));
-  NSX_CUDA(cudaMalloc(&ws.status, sizeof(int)));
-  NSX_CUDA(cudaMalloc(&ws.mask, n));
-  NSX_CUDA(cudaMemcpyAsync(ws.mask, h->lcoef.data(), n, cudaMemcpyHostToDevice, s));
+  // basis (m+1 vectors; the FP64 refinement reuses it for 2*nev rotated vectors), kept by the handle
+  Workspace &ws = workspace(h, m, keep, nev, s);
   Timer tm{h};
   int matvecs = 0, iters = 0, restarts = 0;
   auto V = [&](int j) { return ws.V + (int64_t)j * n; };
@@ -434,11 +617,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
     tm.matvec(V(i), ws.w, prec, s);
     ++matvecs;
     ++iters;
-    dots(ws, ws.V, n, i + 1, ws.w, n, ws.h, false, s);
-    subtract(ws.V, n, i + 1, ws.h, ws.w, n, s);
-    dots(ws, ws.V, n, i + 1, ws.w, n, ws.h2, false, s);  // second Gram-Schmidt pass
-    subtract(ws.V, n, i + 1, ws.h2, ws.w, n, s);
-    dots(ws, ws.w, 0, 1, ws.w, n, ws.h2 + (i + 1), false, s);
+    cgs2(ws, i + 1, ws.h, ws.h2, ws.h2 + (i + 1), s);   // full reorthogonalisation, two passes
     NSX_CUDA(cudaMemcpyAsync(hcol.data(), ws.h, sizeof(double) * (i + 1), cudaMemcpyDeviceToHost, s));
     NSX_CUDA(cudaMemcpyAsync(h2.data(), ws.h2, sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, s));
     NSX_CUDA(cudaStreamSynchronize(s));
@@ -529,8 +708,7 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   for (int c = 0; c < nev; ++c) evals_out[c] = theta[c];
   if (P->refine) {
     // FP64 Rayleigh-Ritz on the Ritz vectors: G = Y^T H Y, eigen-decompose, rotate
-    double *HY = nullptr;
-    NSX_CUDA(cudaMalloc(&HY, sizeof(double) * n * nev));
+    double *HY = ws.HY;
     for (int c = 0; c < nev; ++c) {
       tm.matvec(ws.tmp + (int64_t)c * n, HY + (int64_t)c * n, NSX_FP64, s);
       ++matvecs;
@@ -566,7 +744,6 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
       subtract(ws.tmp + (int64_t)c * n, n, 1, ws.h, ws.w, n, s);
       res[c] = std::sqrt(std::max(host_norm2(ws, ws.w, n, s), 0.0));
     }
-    cudaFree(HY);
     tm.flush();
     nconv = 0;
     for (int c = 0; c < nev; ++c)

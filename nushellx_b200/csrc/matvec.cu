@@ -338,9 +338,11 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
 // of P_r the group's sources are read once into registers (NS of them at most: 16,
 // or ZMAXS when the plan has a larger group) and every operator's mixed row is
 // written to its Zbar slab.
-template <typename T, int NS>
+// TC: the FP32 tensor-core form, Zbar tiles in the MMA's swizzled layout (a row of 128 tile
+// columns is 4 contiguous 128-byte lines, so a warp's store is still one full line).
+template <typename T, int NS, bool TC>
 __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], const int64_t *ysrc, const int64_t *zdst,
-                                        int ns, int na, const T *__restrict__ Y, T *__restrict__ Zb) {
+                                        const int *zk, int ns, int na, const T *__restrict__ Y, T *__restrict__ Zb) {
   const int c = threadIdx.x;
   if (c >= u.ncols) return;
   const int col = u.c0 + c;
@@ -353,18 +355,21 @@ __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], co
       T z = T(0);
 #pragma unroll
       for (int s = 0; s < NS; ++s) z = fma(ws[a][s], y[s], z);
-      Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
+      if constexpr (TC) Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr, c)] = z;
+      else Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
     }
   }
 }
 
-template <typename T, int NS>
+template <typename T, int NS, bool TC>
 __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, const ZGroup *__restrict__ groups,
                                            const ZSrc *__restrict__ srcs, const ZOp *__restrict__ ops,
-                                           const T *__restrict__ W, const T *__restrict__ Y, T *__restrict__ Zb) {
+                                           const ZOpTC *__restrict__ ops_tc, const T *__restrict__ W,
+                                           const T *__restrict__ Y, T *__restrict__ Zb) {
   __shared__ T ws[ZMAXA][ZMAXS];
   __shared__ int64_t ysrc[ZMAXS];
   __shared__ int64_t zdst[ZMAXA];
+  __shared__ int zk[ZMAXA];
   const ZUnit u = units[blockIdx.x];
   const ZGroup G = groups[u.grp];
   const int na = u.op_end - u.op_begin;
@@ -372,10 +377,111 @@ __global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, cons
     const int a = e / ZMAXS, s = e - a * ZMAXS;
     ws[a][s] = s < G.ns ? W[G.w_off + ops[u.op_begin + a].wrow * G.ns + s] : T(0);
   }
-  for (int e = threadIdx.x; e < na; e += blockDim.x) zdst[e] = ops[u.op_begin + e].z;
+  for (int e = threadIdx.x; e < na; e += blockDim.x) {
+    if constexpr (TC) {
+      const ZOpTC o = ops_tc[u.op_begin + e];
+      zdst[e] = o.base + (int64_t)(u.c0 / 128) * o.kgroups * 1024;   // the unit's column tile
+      zk[e] = o.kofs;
+    } else {
+      zdst[e] = ops[u.op_begin + e].z;
+      zk[e] = 0;
+    }
+  }
   for (int e = threadIdx.x; e < ZMAXS; e += blockDim.x) ysrc[e] = e < G.ns ? srcs[G.s_begin + e].y : 0;
   __syncthreads();
-  kz_body<T, NS>(u, ws, ysrc, zdst, G.ns, na, Y, Zb);
+  kz_body<T, NS, TC>(u, ws, ysrc, zdst, zk, G.ns, na, Y, Zb);
+}
+
+// ---------------------------------------------------------------------------
+// k_yz (FP32 form): the neutron-side products fused into the mixing stage, so that Y never
+// goes to HBM.  One CTA per k_z unit (group, P_r, 128-column tile), thread = column.  For
+// each source s = (h, b) of the group the thread forms
+//     Y_s[row, col] = sum_k C_h[row, Q_r col k] rho_b[col - (Q_l col 0), k]
+// for KYZ_RB rows of P_r at a time in registers (the density sub-block (Q_l, Q_r) holding the
+// column comes from a per-CTA column table; C values are shared by the columns of one
+// sub-block and the densities by all rows, so both stay in L1), then writes every proton
+// operator's mixed row sum_s w_(a,s) Y_s to its Zbar tile in the tensor-core layout.  A
+// column no sub-block of a source reaches contributes zero for that source.
+constexpr int KYZ_NS = 16;   // sources per group of the fused stage (larger groups: k_y + k_z)
+constexpr int KYZ_RB = 4;    // rows per register block
+
+__global__ void __launch_bounds__(128) k_yz(const ZUnit *__restrict__ units, const ZGroup *__restrict__ groups,
+                                            const ZSrc *__restrict__ srcs, const ZOp *__restrict__ ops,
+                                            const ZOpTC *__restrict__ ops_tc, const YBlk *__restrict__ blks,
+                                            const float *__restrict__ W, const float *__restrict__ x,
+                                            const float *__restrict__ rho, float *__restrict__ Zb) {
+  __shared__ float ws[ZMAXA][KYZ_NS];
+  __shared__ int64_t zdst[ZMAXA];
+  __shared__ int zk[ZMAXA];
+  __shared__ int16_t colblk[KYZ_NS][128];
+  __shared__ ZSrc ss[KYZ_NS];
+  const ZUnit u = units[blockIdx.x];
+  const ZGroup G = groups[u.grp];
+  const int na = u.op_end - u.op_begin, ns = G.ns;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < na * KYZ_NS; e += blockDim.x) {
+    const int a = e / KYZ_NS, sidx = e - a * KYZ_NS;
+    ws[a][sidx] = sidx < ns ? W[G.w_off + ops[u.op_begin + a].wrow * ns + sidx] : 0.f;
+  }
+  for (int e = tid; e < na; e += blockDim.x) {
+    const ZOpTC o = ops_tc[u.op_begin + e];
+    zdst[e] = o.base + (int64_t)(u.c0 / 128) * o.kgroups * 1024;
+    zk[e] = o.kofs;
+  }
+  for (int e = tid; e < KYZ_NS * 128; e += blockDim.x) (&colblk[0][0])[e] = -1;
+  for (int e = tid; e < ns; e += blockDim.x) ss[e] = srcs[G.s_begin + e];
+  __syncthreads();
+  {  // column -> sub-block tables, 8 threads per source
+    const int sidx = tid >> 3, q = tid & 7;
+    if (sidx < ns) {
+      const ZSrc S = ss[sidx];
+      for (int bi = S.b_begin + q; bi < S.b_end; bi += 8) {
+        const YBlk b = blks[bi];
+        const int lo = max(b.ycol, u.c0), hi = min(b.ycol + b.nl, u.c0 + u.ncols);
+        for (int c = lo; c < hi; ++c) colblk[sidx][c - u.c0] = (int16_t)(bi - S.b_begin);
+      }
+    }
+  }
+  __syncthreads();
+  const int c = tid;
+  if (c >= u.ncols) return;
+  const int col = u.c0 + c;
+  for (int rr0 = 0; rr0 < u.nr; rr0 += KYZ_RB) {
+    const int nrb = min(KYZ_RB, u.nr - rr0);
+    float y[KYZ_NS][KYZ_RB];
+#pragma unroll
+    for (int sidx = 0; sidx < KYZ_NS; ++sidx) {
+#pragma unroll
+      for (int rb = 0; rb < KYZ_RB; ++rb) y[sidx][rb] = 0.f;
+      if (sidx < ns) {
+        const int bi = colblk[sidx][c];
+        if (bi >= 0) {
+          const ZSrc &S = ss[sidx];
+          const YBlk b = blks[S.b_begin + bi];
+          const int64_t m = S.m;
+          const float *cp = x + S.c_base + u.row0 + rr0 + m * b.ccol;
+          const float *rp = rho + b.rho + (col - b.ycol);
+          for (int k = 0; k < b.nr; ++k) {
+            const float rv = __ldg(rp + (int64_t)b.ldr * k);
+#pragma unroll
+            for (int rb = 0; rb < KYZ_RB; ++rb)
+              if (rb < nrb) y[sidx][rb] = fmaf(__ldg(cp + rb + m * k), rv, y[sidx][rb]);
+          }
+        }
+      }
+    }
+    for (int a = 0; a < na; ++a) {
+#pragma unroll
+      for (int rb = 0; rb < KYZ_RB; ++rb) {
+        if (rb < nrb) {
+          float z = 0.f;
+#pragma unroll
+          for (int sidx = 0; sidx < KYZ_NS; ++sidx) z = fmaf(ws[a][sidx], y[sidx][rb], z);
+          Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr0 + rb, c)] = z;
+        }
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -647,8 +753,13 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaEventCreate(&h->ev0));
   NSX_CUDA(cudaEventCreate(&h->ev1));
   // k_a's shared-memory cap: the same constant on every call (harmless to repeat)
-  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<float>::bytes));
   NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<double>::bytes));
+  NSX_CUDA(cudaFuncSetAttribute(k_a_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<16>::SMEM));
+  NSX_CUDA(cudaFuncSetAttribute(k_a_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<32>::SMEM));
+  NSX_CUDA(cudaFuncSetAttribute(k_a_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<48>::SMEM));
+  NSX_CUDA(cudaFuncSetAttribute(k_a_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<64>::SMEM));
+  NSX_CUDA(cudaMalloc(&d.err, sizeof(int)));
+  NSX_CUDA(cudaMemset(d.err, 0, sizeof(int)));
   // copies from pageable memory may return before their DMA lands; work on non-blocking
   // streams (the caller's, or the handle's solve stream) is not ordered after them
   NSX_CUDA(cudaDeviceSynchronize());
@@ -664,13 +775,20 @@ void ensure_precision(nsx_handle *h, int precision) {
     }
   } else if (precision == NSX_FP32) {
     if (!d.y32) {
-      NSX_CUDA(cudaMalloc(&d.y32, ny * sizeof(float)));
-      NSX_CUDA(cudaMalloc(&d.z32, nz * sizeof(float)));
+      // Zbar in the tensor-core tile layout; padding rows and columns stay zero for good.  The
+      // fused FP32 stage forms Y on chip: no Y buffer then.
+      const size_t nz32 = std::max<int64_t>(h->z32_elems, 1);
+      NSX_CUDA(cudaMalloc(&d.y32, (h->max_zns <= KYZ_NS ? 1 : ny) * sizeof(float)));
+      NSX_CUDA(cudaMalloc(&d.z32, nz32 * sizeof(float)));
+      NSX_CUDA(cudaMemset(d.z32, 0, nz32 * sizeof(float)));
+      d.abar_big = dev_copy_pod(h->abar_big);
+      d.abar_small = dev_copy_pod(h->abar_small);
+      d.zops_tc = dev_copy_pod(h->zops_tc);
+      d.atiles_tc = dev_copy_pod(h->atiles_tc);
       d.rhoB32 = dev_copy<float>(h->yrho);
       d.hA32 = dev_copy<float>(h->A.hdense);
       d.hB32 = dev_copy<float>(h->B.hdense);
       d.w32 = dev_copy<float>(h->weights);
-      d.abar32 = dev_copy<float>(h->abar);
       NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
       NSX_CUDA(cudaDeviceSynchronize());  // as in upload()
@@ -727,10 +845,19 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAG
   bytes[1] = es * (n + rhoB + y);                         // C in, rho_B, Y written
   bytes[2] = es * (y + z + (double)h->weights.size());    // Y in, Zbar written
   bytes[3] = es * (z + (double)h->abar.size() + 2.0 * n); // Zbar in, Abar, out read + written
+  const bool fused = precision == NSX_FP32 && h->max_zns <= KYZ_NS;
+  if (precision == NSX_FP32) {   // tensor-core layout of Zbar, split Abar
+    bytes[2] = es * (y + (double)h->z32_elems + (double)h->weights.size());
+    bytes[3] = es * ((double)h->z32_elems + 2.0 * (double)h->abar_big.size() + 2.0 * n);
+  }
+  if (fused) {   // k_yz: C and rho_B in, Zbar written; Y never stored
+    bytes[1] = 0.0;
+    bytes[2] = es * (n + rhoB + (double)h->z32_elems + (double)h->weights.size());
+  }
   bytes[4] = precision == NSX_FP64 ? 0.0 : n * (8.0 + 4.0);
   flops[0] = h->flops_like;
-  flops[1] = h->flops_y;
-  flops[2] = h->flops_mix;
+  flops[1] = fused ? 0.0 : h->flops_y;
+  flops[2] = fused ? h->flops_y + h->flops_mix : h->flops_mix;
   flops[3] = h->flops_a;
   flops[4] = 0.0;
 }
@@ -743,19 +870,49 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoB, const T
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
   }
-  if (!h->ygroups.empty()) {
-    StageScope sc(h, 1, s);
-    k_y<T><<<(unsigned)h->ygroups.size(), 128, 0, s>>>(d.ygroups, d.yblks, x, rhoB, Y);
+  constexpr bool TC = std::is_same<T, float>::value;   // FP32: proton side on the tensor cores
+  const bool fused = TC && h->max_zns <= KYZ_NS;          // FP32: Y formed inside the mixing stage
+  if (fused) {
+    if (!h->zunits.empty()) {
+      StageScope sc(h, 2, s);
+      k_yz<<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, d.yblks,
+                                                       reinterpret_cast<const float *>(w),
+                                                       reinterpret_cast<const float *>(x),
+                                                       reinterpret_cast<const float *>(rhoB),
+                                                       reinterpret_cast<float *>(Z));
+    }
+  } else {
+    if (!h->ygroups.empty()) {
+      StageScope sc(h, 1, s);
+      k_y<T><<<(unsigned)h->ygroups.size(), 128, 0, s>>>(d.ygroups, d.yblks, x, rhoB, Y);
+    }
+    if (!h->zunits.empty()) {
+      StageScope sc(h, 2, s);
+      // sources per group: registers for 16 unless the plan has a larger group
+      if (h->max_zns <= 16)
+        k_z<T, 16, TC><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc,
+                                                                   w, Y, Z);
+      else
+        k_z<T, ZMAXS, TC><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops,
+                                                                      d.zops_tc, w, Y, Z);
+    }
   }
-  if (!h->zunits.empty()) {
-    StageScope sc(h, 2, s);
-    // sources per group: registers for 16 unless the plan has a larger group
-    if (h->max_zns <= 16)
-      k_z<T, 16><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
-    else
-      k_z<T, ZMAXS><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, w, Y, Z);
-  }
-  if (!h->atiles.empty()) {
+  if constexpr (TC) {
+    for (int c = 0; c < KTC_NCLASS; ++c) {
+      const int64_t n = h->atc_off[c + 1] - h->atc_off[c];
+      if (n == 0) continue;
+      StageScope sc(h, 3, s);
+      const ATileTC *tl = d.atiles_tc + h->atc_off[c];
+      float *o = reinterpret_cast<float *>(out);
+      const float *zf = reinterpret_cast<const float *>(Z);
+      switch (c) {
+        case 0: k_a_tc<16><<<(unsigned)n, 128, KaTcCfg<16>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
+        case 1: k_a_tc<32><<<(unsigned)n, 128, KaTcCfg<32>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
+        case 2: k_a_tc<48><<<(unsigned)n, 128, KaTcCfg<48>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
+        default: k_a_tc<64><<<(unsigned)n, 128, KaTcCfg<64>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
+      }
+    }
+  } else if (!h->atiles.empty()) {
     StageScope sc(h, 3, s);
     k_a<T><<<(unsigned)h->atiles.size(), 128, KaSmem<T>::bytes, s>>>(d.atiles, abar, Z, out);
   }
@@ -776,7 +933,7 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       StageScope sc(h, 4, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float>(h, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32, d.y32, d.z32, s);
+    run_stages<float>(h, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, nullptr, d.y32, d.z32, s);
     {
       StageScope sc(h, 4, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
@@ -794,9 +951,23 @@ void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double 
   run_stages<double>(h, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
 }
 
+// Fails with NSX_E_CUDA if a tensor-core kernel gave up a bounded wait since the last check
+// (the word is cleared).  Synchronises the device.
+void check_device_error(nsx_handle *h) {
+  if (!h->d.err) return;
+  int e = 0;
+  NSX_CUDA(cudaMemcpy(&e, h->d.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    NSX_CUDA(cudaMemset(h->d.err, 0, sizeof(int)));
+    fail(NSX_E_CUDA, "a tensor-core kernel gave up waiting for its operands (bounded wait); results are invalid");
+  }
+}
+
 void release(nsx_handle *h) {
+  release_lanczos(h);
   auto &d = h->d;
   void *ptrs[] = {d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
+                  d.abar_big, d.abar_small, d.zops_tc, d.atiles_tc, d.err,
                   d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zops, d.atiles, d.ltiles,
                   d.y64, d.z64, d.y32, d.z32, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)

@@ -7,6 +7,7 @@
 #include <unordered_map>
 #include <cuda_runtime.h>
 #include "nsx.h"
+#include "ka_tc.cuh"
 
 namespace nsx {
 
@@ -118,6 +119,10 @@ struct ZGroup {
 };
 struct ZSrc {
   int64_t y;                // offset of the source's Y matrix
+  int64_t c_base;           // offset of the source's input block h (the fused stage forms Y itself)
+  int32_t m;                // d_ar (leading dimension of C_h)
+  int32_t b_begin, b_end;   // the Y matrix's density sub-blocks in yblks (ascending ycol)
+  int32_t pad;
 };
 struct ZUnit {              // (group, P_r, column tile)
   int32_t grp;
@@ -151,6 +156,16 @@ struct ATile {
   int64_t zbar;     // offset of Zbar[0, col0]
   int64_t abar;     // offset of Abar[0, 0] of the slab
 };
+// FP32 form on the tensor cores (k_a_tc): the mixing stage writes each Zbar tile (slab,
+// 128-column tile) in the MMA's MN-major swizzled layout; a ZOpTC gives the operator's slab
+// (base of its tile 0, tiles kgroups * 1024 floats apart) and its first stacked row.
+struct ZOpTC {
+  int64_t base;     // float offset of the slab's Zbar tile 0
+  int32_t kofs;     // first stacked row of the operator's rows
+  int32_t kgroups;  // the slab's stacked rows / 8 (padded)
+};
+constexpr int KTC_NCLASS = 4;   // N padded to 16, 32, 48, 64 (nl of the proton partition)
+
 // like-particle part: out_blk = Ha C + C Hb, 64x64 output tiles.
 struct LTile {
   int64_t c;        // block offset
@@ -166,6 +181,10 @@ struct DeviceBuffers {
   float *rhoB32 = nullptr, *hA32 = nullptr, *hB32 = nullptr, *w32 = nullptr;
   double *abar = nullptr;
   float *abar32 = nullptr;
+  float *abar_big = nullptr, *abar_small = nullptr;   // k_a_tc operands (TF32 split)
+  ZOpTC *zops_tc = nullptr;
+  ATileTC *atiles_tc = nullptr;                       // all classes, class c from atc_off[c]
+  int *err = nullptr;                                 // kernels' error word (bounded waits)
   YGroup *ygroups = nullptr;
   YBlk *yblks = nullptr;
   ZGroup *zgroups = nullptr;
@@ -205,6 +224,12 @@ struct nsx_handle {
   std::vector<nsx::ZOp> zops;
   std::vector<nsx::ATile> atiles;
   std::vector<double> abar;
+  // FP32 tensor-core form of the proton side
+  std::vector<nsx::ZOpTC> zops_tc;      // parallel to zops
+  std::vector<nsx::ATileTC> atiles_tc;  // grouped by N class, longest first in each
+  int64_t atc_off[nsx::KTC_NCLASS + 1] = {};
+  std::vector<float> abar_big, abar_small;
+  int64_t z32_elems = 0;
   std::vector<double> yrho;        // padded neutron densities read by the Y stage
   std::vector<double> weights;
   std::vector<nsx::LTile> ltiles;
@@ -221,9 +246,27 @@ struct nsx_handle {
   bool timing = false;
   int last_precision = NSX_FP64;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
+  void *lws = nullptr;   // the Lanczos solver's device workspace (lanczos.cu), kept between solves
 };
 
 namespace nsx {
+// Terms of a compressed pn interaction read from a .dop file (compress.cpp).
+struct DopArrays {
+  std::vector<int32_t> lam2, parity, eig;
+  std::vector<double> e, u;
+  std::vector<uint8_t> shells;
+  nsx_dop view() {
+    nsx_dop d;
+    d.nterms = (int32_t)e.size();
+    d.lam2 = lam2.data();
+    d.parity = parity.data();
+    d.eig = eig.data();
+    d.e = e.data();
+    d.shells = shells.data();
+    d.u = u.data();
+    return d;
+  }
+};
 // Offset of Zbar in a caller-provided FP64 scratch buffer that holds Y then Zbar: Y's length
 // rounded up to 32 elements, so that Zbar starts on a 256-byte boundary (k_a copies its rows
 // with 16-byte asynchronous copies).
@@ -240,6 +283,8 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
 void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s);
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]);
 void flush_stage_events(nsx_handle *h);
+void check_device_error(nsx_handle *h);
+void release_lanczos(nsx_handle *h);
 void write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs, int nev,
                    int iterations, const char *intfile, int T2);
 double sixj(int a, int b, int c, int d, int e, int f);

@@ -301,35 +301,53 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       }
     }
   }
-  // ---- Y operands: one row-major d_ar x d_bl matrix per (input block h, neutron key b) ----
-  std::map<std::pair<int, int>, int> ymat;
-  std::vector<std::pair<int, int>> ymats;
+  // ---- Y operands: one row-major d_ar x d_bl matrix per (input block h, neutron key b, layer) ----
+  // A layer of a neutron density holds at most one sub-block per left partition (the Y stage
+  // gives each output column one sub-block).  The densities of the reference's files have one
+  // layer; combined operators (the compressed interaction) sum several densities and get one
+  // layer per sub-block of a left partition, each a source of its own with the same weight.
+  std::vector<std::vector<int>> blayer(B.keys.size());
+  std::vector<int> nlayer(B.keys.size(), 1);
+  for (size_t bk = 0; bk < B.keys.size(); ++bk) {
+    std::map<int, int> seen;   // left partition -> sub-blocks so far
+    for (const RhoBlk &rb : B.kblocks[bk]) {
+      const int L = seen[rb.pl]++;
+      blayer[bk].push_back(L);
+      nlayer[bk] = std::max(nlayer[bk], L + 1);
+    }
+  }
+  std::map<std::tuple<int, int, int>, int> ymat;
+  std::vector<std::tuple<int, int, int>> ymats;
   std::vector<int64_t> yoff;
   int64_t ytot = 0;
-  auto get_ymat = [&](int hb, int bk) {
-    auto it = ymat.find({hb, bk});
+  auto get_ymat = [&](int hb, int bk, int L) {
+    auto it = ymat.find({hb, bk, L});
     if (it != ymat.end()) return it->second;
     int id = (int)ymats.size();
-    ymat[{hb, bk}] = id;
-    ymats.push_back({hb, bk});
+    ymat[{hb, bk, L}] = id;
+    ymats.push_back({hb, bk, L});
     yoff.push_back(ytot);
     ytot += (int64_t)h->blocks[hb].da * B.dim((int)(B.keys[bk] & 255));
     return id;
   };
   for (const Row &r : table)
-    for (const Entry &e : r.e) get_ymat(e.hb, e.bk);
+    for (const Entry &e : r.e)
+      for (int L = 0; L < nlayer[e.bk]; ++L) get_ymat(e.hb, e.bk, L);
   h->ygroups.clear();
   h->yblks.clear();
   h->yrho.clear();
   h->flops_y = 0;
   std::unordered_map<int64_t, int64_t> yrho_at;  // .trd value offset -> padded offset
+  std::vector<int32_t> ymat_b0(ymats.size()), ymat_b1(ymats.size());
   for (size_t y = 0; y < ymats.size(); ++y) {
-    int hb = ymats[y].first, bk = ymats[y].second;
+    const int hb = std::get<0>(ymats[y]), bk = std::get<1>(ymats[y]), layer = std::get<2>(ymats[y]);
     const Block &ib = h->blocks[hb];
     int J2bl = (int)(B.keys[bk] & 255), J2br = (int)((B.keys[bk] >> 8) & 255);
     int b0 = (int)h->yblks.size();
     double nnz = 0;
-    for (const RhoBlk &rb : B.kblocks[bk]) {
+    for (size_t bi = 0; bi < B.kblocks[bk].size(); ++bi) {
+      if (blayer[bk][bi] != layer) continue;
+      const RhoBlk &rb = B.kblocks[bk][bi];
       YBlk yb;
       yb.ccol = B.poff[B.jidx(J2br)][rb.pr];
       yb.ycol = B.poff[B.jidx(J2bl)][rb.pl];
@@ -355,6 +373,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       if (h->yblks[i].ycol < h->yblks[i - 1].ycol + h->yblks[i - 1].nl)
         fail(NSX_E_ARG, "neutron density sub-blocks of one operator overlap in their left partition");
     h->flops_y += 2.0 * ib.da * nnz;
+    ymat_b0[y] = b0;
+    ymat_b1[y] = b1;
     for (int r0 = 0; r0 < ib.da; r0 += KY_TILE_ROWS)
       h->ygroups.push_back({ib.off, yoff[y], ib.da, r0, b0, b1, B.dim(J2bl), 0});
   }
@@ -393,35 +413,41 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     const int bl = std::get<0>(gk.first), jar = std::get<1>(gk.first);
     const Block &ob = h->blocks[bl];
     const std::vector<int> &rows = gk.second;
-    std::map<std::pair<int, int>, int> sidx;
-    std::vector<std::pair<int, int>> srcs;
+    std::map<std::tuple<int, int, int>, int> sidx;
+    std::vector<std::tuple<int, int, int>> srcs;
     for (int r : rows)
       for (const Entry &e : table[r].e)
-        if (!sidx.count({e.hb, e.bk})) {
-          sidx[{e.hb, e.bk}] = (int)srcs.size();
-          srcs.push_back({e.hb, e.bk});
-        }
+        for (int L = 0; L < nlayer[e.bk]; ++L)
+          if (!sidx.count({e.hb, e.bk, L})) {
+            sidx[{e.hb, e.bk, L}] = (int)srcs.size();
+            srcs.push_back({e.hb, e.bk, L});
+          }
     // sub-groups of at most ZMAXS sources; each has its own stacked rows (the proton density
     // block is repeated in Abar), so no two k_z units write the same Zbar row
     for (size_t s0 = 0; s0 < srcs.size(); s0 += ZMAXS) {
       const size_t s1 = std::min(srcs.size(), s0 + (size_t)ZMAXS);
       ZGroup G;
       G.s_begin = (int)h->zsrcs.size();
-      for (size_t si = s0; si < s1; ++si) h->zsrcs.push_back({yoff[get_ymat(srcs[si].first, srcs[si].second)]});
+      for (size_t si = s0; si < s1; ++si) {
+        const int ym = get_ymat(std::get<0>(srcs[si]), std::get<1>(srcs[si]), std::get<2>(srcs[si]));
+        const Block &ib = h->blocks[std::get<0>(srcs[si])];
+        h->zsrcs.push_back({yoff[ym], ib.off, ib.da, ymat_b0[ym], ymat_b1[ym], 0});
+      }
       G.s_end = (int)h->zsrcs.size();
       G.ns = (int)(s1 - s0);
       G.w_off = (int)h->weights.size();
       std::vector<char> active(rows.size(), 0);  // operators with a source in this sub-group
       for (size_t ai = 0; ai < rows.size(); ++ai) {
         std::vector<double> wr(G.ns, 0.0);
-        for (const Entry &e : table[rows[ai]].e) {
-          int si = sidx[{e.hb, e.bk}];
-          if (si >= (int)s0 && si < (int)s1) {
-            wr[si - s0] += e.w;
-            h->wterms.push_back({(int64_t)G.w_off + (int64_t)ai * G.ns + (si - (int)s0), e.op, e.rw});
-            active[ai] = 1;
+        for (const Entry &e : table[rows[ai]].e)
+          for (int L = 0; L < nlayer[e.bk]; ++L) {
+            int si = sidx[{e.hb, e.bk, L}];
+            if (si >= (int)s0 && si < (int)s1) {
+              wr[si - s0] += e.w;
+              h->wterms.push_back({(int64_t)G.w_off + (int64_t)ai * G.ns + (si - (int)s0), e.op, e.rw});
+              active[ai] = 1;
+            }
           }
-        }
         h->weights.insert(h->weights.end(), wr.begin(), wr.end());
       }
       const int gid = (int)h->zgroups.size();
@@ -458,6 +484,18 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     zoff[sl] = ztot;
     ztot += (int64_t)slabK[sl] * padz(h->blocks[slabs[sl].first].db);
   }
+  // FP32 tensor-core layout: per slab, ceil(d_bl / 128) tiles of kgroups * 1024 floats
+  std::vector<int64_t> ztc(slabs.size());
+  std::vector<int32_t> kgr(slabs.size());
+  int64_t ztc_tot = 0;
+  for (size_t sl = 0; sl < slabs.size(); ++sl) {
+    kgr[sl] = (slabK[sl] + 7) / 8;
+    ztc[sl] = ztc_tot;
+    const int db = h->blocks[slabs[sl].first].db;
+    ztc_tot += (int64_t)((db + 127) / 128) * kgr[sl] * 1024;
+  }
+  h->z32_elems = ztc_tot;
+  h->zops_tc.clear();
   // k_z units: (group, P_r, 128-column tile)
   const int ZT = 128;
   for (auto &pd : pending) {
@@ -465,7 +503,10 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
     const Block &ob = h->blocks[bl];
     int op0 = (int)h->zops.size();
     const int ldz = (int)padz(ob.db);
-    for (const PendingOp &o : pd.ops) h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ldz, o.wrow, 0});
+    for (const PendingOp &o : pd.ops) {
+      h->zops.push_back({zoff[o.slab] + (int64_t)o.kofs * ldz, o.wrow, 0});
+      h->zops_tc.push_back({ztc[o.slab], o.kofs, kgr[o.slab]});
+    }
     int op1 = (int)h->zops.size();
     for (int c0 = 0; c0 < ob.db; c0 += ZT) {
       ZUnit u;
@@ -517,6 +558,52 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   std::stable_sort(h->atiles.begin(), h->atiles.end(), [](const ATile &x, const ATile &y) {
     return (int64_t)(x.k_end - x.k_begin) * x.nl > (int64_t)(y.k_end - y.k_begin) * y.nl;
   });
+  // FP32 tensor-core tiles: Abar^T packed K-major per slab (TF32 big and small parts), one
+  // tile per (slab, 128-column tile), grouped by N = nl padded to 16 and longest first
+  h->abar_big.clear();
+  h->abar_small.clear();
+  std::vector<std::vector<ATileTC>> tcls(KTC_NCLASS);
+  for (size_t sl = 0; sl < slabs.size(); ++sl) {
+    const int bl = slabs[sl].first, pl = slabs[sl].second;
+    const Block &ob = h->blocks[bl];
+    const int nl = A.njt_of(pl, ob.J2a);
+    if (nl > 16 * KTC_NCLASS) continue;   // refused in upload (k_a's limit)
+    const int npad = (nl + 15) / 16 * 16;
+    const int kg = kgr[sl];
+    if (kg == 0) continue;
+    const int64_t at = (int64_t)h->abar_big.size();
+    h->abar_big.resize(at + (int64_t)kg * 8 * npad, 0.f);
+    h->abar_small.resize(at + (int64_t)kg * 8 * npad, 0.f);
+    int k = 0;
+    for (auto &bv : slab_blocks[sl])   // (nr, offset of the nl x nr density block)
+      for (int kk = 0; kk < bv.first; ++kk, ++k)
+        for (int l = 0; l < nl; ++l) {
+          const float x = (float)A.vals[bv.second + (int64_t)nl * kk + l];
+          const float b = umma::tf32_big(x);
+          const int64_t e = at + umma::b_kmajor_index(l, k, npad);
+          h->abar_big[e] = b;
+          h->abar_small[e] = x - b;
+        }
+    for (int t = 0; t * 128 < ob.db; ++t) {
+      ATileTC u;
+      u.zbar = ztc[sl] + (int64_t)t * kg * 1024;
+      u.abar = at;
+      u.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)t * 128 * ob.da;
+      u.kgroups = kg;
+      u.ld = ob.da;
+      u.nl = nl;
+      u.ncols = std::min(128, ob.db - t * 128);
+      tcls[npad / 16 - 1].push_back(u);
+    }
+  }
+  h->atiles_tc.clear();
+  for (int c = 0; c < KTC_NCLASS; ++c) {
+    std::stable_sort(tcls[c].begin(), tcls[c].end(),
+                     [](const ATileTC &x, const ATileTC &y) { return x.kgroups > y.kgroups; });
+    h->atc_off[c] = (int64_t)h->atiles_tc.size();
+    h->atiles_tc.insert(h->atiles_tc.end(), tcls[c].begin(), tcls[c].end());
+  }
+  h->atc_off[KTC_NCLASS] = (int64_t)h->atiles_tc.size();
   h->z_elems = ztot;
   h->y_elems = ytot;
   h->max_ynl = h->max_ynr = h->max_anl = h->max_ldy = 0;

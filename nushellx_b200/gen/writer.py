@@ -142,19 +142,23 @@ def write_trd(path, S, rho, max_j2):
                 w.write(d["masks"][k].astype("<u4").view("<i4"))
 
 
-def write_oph(path, vlam, norb):
+def write_oph(path, vlam, norb, parity=None):
+    """The pn multipole file; pl / pr are the parities of the operator's two orbit pairs
+    (p1*p3 and p2*p4, src/NuOp/NuOp.f90:378-379); parity: +1/-1 per orbit (all +1 if None)."""
+    par = parity if parity is not None else [1] * norb
     recs = []
     max_lmo = 0
     # both species orders, as NuOp writes them (pnnp = 0 and 1, NuOp.f90:240-262)
     for (o1, o3, o2, o4, lam), v in vlam.items():
         max_lmo = max(max_lmo, lam)
-        recs.append((bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]), v))
-        recs.append((bytes([norb + o1 + 1, norb + o3 + 1, o2 + 1, o4 + 1, lam, 0, 0, 0]), v))
+        pl, pr = par[o1] * par[o3], par[o2] * par[o4]
+        recs.append((bytes([o1 + 1, o3 + 1, norb + o2 + 1, norb + o4 + 1, lam, 0, 0, 0]), v, pl, pr))
+        recs.append((bytes([norb + o1 + 1, norb + o3 + 1, o2 + 1, o4 + 1, lam, 0, 0, 0]), v, pl, pr))
     recs.sort()
     with RecordWriter(path) as w:
         w.write(i4(len(recs), max_lmo))
-        for kb, v in recs:
-            w.write(kb, r8(v), i4(1), i4(1))
+        for kb, v, pl, pr in recs:
+            w.write(kb, r8(v), i4(pl), i4(pr))
 
 
 def write_spe(path, spe, renorm, no_level, restart=None):
@@ -189,8 +193,9 @@ def write_like(prefix_for_J, S, segs):
             w.write(i4(len(lst), S.dimJ(J2)), r4(X_STAMP))
 
 
-def write_problem(P, outdir, tag, no_level=10):
-    """Write all input files of problem P under outdir; returns the manifest dict."""
+def write_problem(P, outdir, tag, no_level=10, dop_cut=None):
+    """Write all input files of problem P under outdir; returns the manifest dict.  With
+    dop_cut = (cut, cutm) also the compressed interaction <tag>i.dop of NuDiop (gen/dop.py)."""
     os.makedirs(outdir, exist_ok=True)
     A, B = P.A, P.B
     norb = P.space.norb
@@ -199,7 +204,7 @@ def write_problem(P, outdir, tag, no_level=10):
     write_trd(base + "a.trd", A, P.rhoA, 2 * max(P.space.j2))
     write_tri(base + "b.tri", B, False)
     write_trd(base + "b.trd", B, P.rhoB, 2 * max(P.space.j2))
-    write_oph(base + "i.oph", P.vlam, norb)
+    write_oph(base + "i.oph", P.vlam, norb, P.space.parity)
     write_spe(base + "i.spe", P.space.spe, P.renorm, no_level)
     la = like_file_names(base + "a", A, -A.n, "x")
     lb = like_file_names(base + "b", B, B.n, "x")
@@ -211,6 +216,10 @@ def write_problem(P, outdir, tag, no_level=10):
         "shell_parity": list(P.space.parity) * 2,
         "no_state": P.no_state, "nblocks": len(P.blocks),
     }
+    if dop_cut is not None:
+        from .dop import diop, write_dop
+        write_dop(base + "i.dop", diop(P.vlam, P.space, *dop_cut))
+        man["dop"] = base + "i.dop"
     with open(base + ".json", "w") as f:
         json.dump(man, f, indent=1)
     return man

@@ -73,9 +73,28 @@ class Files(C.Structure):
                 ("nshells", C.c_int32), ("nshells_p", C.c_int32), ("shell_parity", _p(C.c_int32))]
 
 
+class Dop(C.Structure):
+    _fields_ = [("nterms", C.c_int32), ("lam2", _p(C.c_int32)), ("parity", _p(C.c_int32)), ("eig", _p(C.c_int32)),
+                ("e", _p(C.c_double)), ("shells", _p(C.c_uint8)), ("u", _p(C.c_double))]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("y_elems", C.c_int64), ("zbar_elems", C.c_int64), ("zbar_tc_elems", C.c_int64),
+                ("y_row_tiles_max", C.c_int32), ("group_sources_max", C.c_int32), ("fused_fp32", C.c_int32),
+                ("slab_rows_max", C.c_int32), ("slab_splits_max", C.c_int32), ("slab_nl_max", C.c_int32),
+                ("tc_tiles", C.c_int64 * 4), ("tc_chunks_max", C.c_int64)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "tc_tiles"}
+        d["tc_tiles"] = [self.tc_tiles[i] for i in range(4)]
+        return d
+
+
 SYMBOLS = {
     "nsx_create": (C.c_int, [_p(Problem), C.c_int, _p(C.c_void_p)]),
     "nsx_load_files": (C.c_int, [_p(Files), C.c_int, _p(C.c_void_p)]),
+    "nsx_load_files_z": (C.c_int, [_p(Files), C.c_char_p, C.c_int, _p(C.c_void_p)]),
+    "nsx_create_z": (C.c_int, [_p(Problem), _p(Dop), C.c_int, _p(C.c_void_p)]),
     "nsx_file_code": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p]),
     "nsx_set_interaction": (C.c_int, [C.c_void_p, _p(C.c_double), C.c_int32, _p(C.c_double), C.c_int64,
                                       _p(C.c_double), C.c_int64]),
@@ -92,6 +111,7 @@ SYMBOLS = {
                                   _p(_p(C.c_double)), _p(Report)]),
     "nsx_write_results": (C.c_int, [C.c_void_p, C.c_char_p, _p(C.c_double), _p(C.c_double), C.c_int32, C.c_int32,
                                     C.c_char_p, C.c_int32]),
+    "nsx_get_plan_info": (C.c_int, [C.c_void_p, _p(PlanInfo)]),
     "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
     "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
     "nsx_destroy": (None, [C.c_void_p]),
@@ -228,8 +248,33 @@ class Solver:
         return cls(h, lib)
 
     @classmethod
-    def from_files(cls, manifest, device=0):
-        """From the reference-format files described by a generator manifest (dict or .json path)."""
+    def from_problem_z(cls, P, dop_entries, device=0):
+        """From an in-memory problem with NuTRLZ's compressed pn interaction (nsx_create_z);
+        dop_entries as gen.dop.diop() returns them."""
+        lib = load_library()
+        prob, keep = build_problem_struct(P)
+        rows = [(lam, par, i + 1, e, sh, u) for lam, par, kept in dop_entries
+                for i, (e, comps) in enumerate(kept) for (*sh, u) in comps]
+        arr = dict(lam2=np.array([r[0] for r in rows], dtype=np.int32),
+                   par=np.array([r[1] for r in rows], dtype=np.int32),
+                   eig=np.array([r[2] for r in rows], dtype=np.int32),
+                   e=np.array([r[3] for r in rows], dtype=np.float64),
+                   sh=np.array([r[4] for r in rows], dtype=np.uint8).ravel(),
+                   u=np.array([r[5] for r in rows], dtype=np.float64))
+        d = Dop()
+        d.nterms = len(rows)
+        d.lam2, d.parity, d.eig = (_ptr(arr[k], C.c_int32) for k in ("lam2", "par", "eig"))
+        d.e, d.u = _ptr(arr["e"], C.c_double), _ptr(arr["u"], C.c_double)
+        d.shells = _ptr(arr["sh"], C.c_uint8)
+        h = C.c_void_p()
+        _check(lib.nsx_create_z(C.byref(prob), C.byref(d), device, C.byref(h)))
+        return cls(h, lib)
+
+    @classmethod
+    def from_files(cls, manifest, device=0, dop=None):
+        """From the reference-format files described by a generator manifest (dict or .json path);
+        with dop (a .dop path) the pn product uses NuTRLZ's compressed interaction
+        (nsx_load_files_z)."""
         lib = load_library()
         if isinstance(manifest, str):
             with open(manifest) as f:
@@ -245,7 +290,10 @@ class Solver:
         f.nshells, f.nshells_p = 2 * m["norb"], m["norb"]
         f.shell_parity = sp.ctypes.data_as(_p(C.c_int32))
         h = C.c_void_p()
-        _check(lib.nsx_load_files(C.byref(f), device, C.byref(h)))
+        if dop is None:
+            _check(lib.nsx_load_files(C.byref(f), device, C.byref(h)))
+        else:
+            _check(lib.nsx_load_files_z(C.byref(f), dop.encode(), device, C.byref(h)))
         return cls(h, lib)
 
     # -- operations -----------------------------------------------------------------
@@ -332,6 +380,12 @@ class Solver:
 
     def stats_reset(self, timing=False):
         _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))
+
+    def plan_info(self):
+        """Which H.v kernel paths this handle's products take (nsx_get_plan_info)."""
+        pi = PlanInfo()
+        _check(self._lib.nsx_get_plan_info(self._h, C.byref(pi)))
+        return pi.as_dict()
 
     def stats(self):
         st = Stats()

@@ -148,6 +148,7 @@ class Oracle:
         r = _records(man["int"] + ".oph")
         nop = struct.unpack_from("<i", r[0], 0)[0]
         renorm = float(open(man["int"] + ".spe").read().split("\n")[1])
+        self.renorm = renorm
         self.vop = {}
         for rec in r[1:1 + nop]:
             key = tuple(rec[:5])
@@ -227,3 +228,92 @@ class Oracle:
                 f += 2.0 * self.A.dim(self.blocks[hb][0]) * self.B.rho[kb].nnz
             f += 2.0 * dbl * self.A.rho[ka].nnz
         return f
+
+
+def read_dop_terms(path):
+    """The .dop file of NuDiop (list-directed text): {(2lam, parity, eigenvector number): (e, [(s1, s3,
+    s2, s4, u), ...])} -- the layout read by src/NuTRLZ/NuCoreXZ.f90:1637-1650."""
+    tok = open(path).read().split()
+    p = [0]
+
+    def nxt(f=int):
+        p[0] += 1
+        return f(tok[p[0] - 1])
+
+    out = {}
+    max_lmo = nxt()
+    for _ in range(2 * (max_lmo // 2 + 1)):
+        lam, par, nel = nxt(), nxt(), nxt()
+        for i in range(1, nel + 1):
+            e, nle = nxt(float), nxt()
+            comps = [(nxt(), nxt(), nxt(), nxt(), nxt(float)) for _ in range(nle)]
+            out[(lam, par, i)] = (e, comps)
+    return out
+
+
+class OracleZ(Oracle):
+    """H.v with NuTRLZ's compressed pn interaction (src/NuTRLZ/NuCoreXZ.f90:1613-1887 prd, table
+    :1475-1611): the densities folded into combined operators, proton e*renorm*u_e(a)*rho_a and
+    neutron u_e(b)*rho_b, paired by equal (2lam, parity, e) with the Racah weight alone."""
+
+    def __init__(self, man, dop_path):
+        super().__init__(man)
+        A, B, J2 = self.A, self.B, self.J2
+        terms = read_dop_terms(dop_path)
+        comb_a, comb_b = {}, {}
+        for (lam, par, i), (e, comps) in terms.items():
+            for ja in range(A.minJ2, A.maxJ2 + 1, 2):
+                for jr in range(A.minJ2, A.maxJ2 + 1, 2):
+                    M = None
+                    for s1, s3, s2, s4, u in comps:
+                        r = A.rho.get((ja, jr, s1, s3, lam))
+                        if r is not None:
+                            M = (e * self.renorm * u) * r if M is None else M + (e * self.renorm * u) * r
+                    if M is not None:
+                        comb_a[(ja, jr, lam, par, i)] = M.tocsr()
+            for jb in range(B.minJ2, B.maxJ2 + 1, 2):
+                for jr in range(B.minJ2, B.maxJ2 + 1, 2):
+                    M = None
+                    for s1, s3, s2, s4, u in comps:
+                        r = B.rho.get((jb, jr, s2, s4, lam))
+                        if r is not None:
+                            M = u * r if M is None else M + u * r
+                    if M is not None:
+                        comb_b[(jb, jr, lam, par, i)] = M.tocsr()
+        bidx = {b: i for i, b in enumerate(self.blocks)}
+        self.table = []
+        self.rho_a_z, self.rho_b_z = comb_a, comb_b
+        for bl, (jal, jbl) in enumerate(self.blocks):
+            for ka in comb_a:
+                if ka[0] != jal:
+                    continue
+                jar = ka[1]
+                ents = []
+                for kb in comb_b:
+                    if kb[0] != jbl or kb[2:] != ka[2:]:
+                        continue
+                    hb = bidx.get((jar, kb[1]))
+                    if hb is None:
+                        continue
+                    w = racah_weight(jal, jbl, jar, kb[1], J2, ka[2])
+                    if w != 0.0:
+                        ents.append((kb, hb, w))
+                if ents:
+                    self.table.append((bl, ka, ents))
+
+    def matvec(self, x):
+        x = np.asarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        A, B = self.A, self.B
+        for k, (ja, jb) in enumerate(self.blocks):
+            C = self.block(x, k)
+            if C.size == 0:
+                continue
+            y[self.off[k]:self.off[k + 1]] = (A.H[ja] @ C + C @ B.H[jb]).T.ravel()
+        for bl, ka, ents in self.table:
+            T = None
+            for kb, hb, w in ents:
+                t = w * (self.rho_b_z[kb] @ self.block(x, hb).T).T
+                T = t if T is None else T + t
+            y[self.off[bl]:self.off[bl + 1]] += np.asarray(self.rho_a_z[ka] @ T).T.ravel()
+        return y

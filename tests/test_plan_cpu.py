@@ -88,3 +88,16 @@ def test_output_files_round_trip_without_a_gpu(name, tmp_path):
     r2 = struct.unpack("<iifiiiiiiii", read_records(prefix + ".abz")[1])
     assert r2[0] == 123
     S.close()
+
+
+def test_plan_reaches_the_kernel_paths_the_gpu_tests_rely_on():
+    """The plan statistics behind the GPU path tests (no GPU needed: plan-only handles)."""
+    from conftest import custom_problem
+    from nushellx_b200.nsx import Solver
+    from test_matvec_gpu import PATH_CASES, check_paths
+    for name, case in PATH_CASES.items():
+        S = Solver.from_problem(custom_problem(*case), device=-1)
+        check_paths(name, S.plan_info())
+        S.close()
+    info = Solver.from_problem(make_problem("fp_4p4n_0"), device=-1).plan_info()
+    assert info["fused_fp32"] == 1 and info["slab_splits_max"] > 1
