@@ -192,6 +192,16 @@ int nsx_matvec_noalloc(nsx_handle *h, const double *x, double *y, void *stream);
 /* The same with HOST pointers: copies in, multiplies, copies out, synchronises. */
 int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision);
 
+/* <psi_i|H|psi_j> between nvec host vectors (vecs: [nvec][no_state], at most 64): the
+ * matrix NuXpct forms between stored eigenvectors (src/NuXpct/NuCoreXE.f90:1417-1471),
+ * matrixc(i, j) = (H psi_i) . psi_j, returned column-major in out[nvec][nvec]
+ * (out[i + nvec*j]).  For eigenvectors it is diagonal with the eigenvalues on it. */
+int nsx_expectation_matrix(nsx_handle *h, const double *vecs, int32_t nvec, int32_t precision, double *out);
+/* The same on files, as NuXpct runs: the levels of the .xvc file at xvc_path (NuVec's
+ * eigenvector file) in, <out_prefix>.ovl (text, 8f10.4 per column) and <out_prefix>.ovx
+ * (unformatted: no_levels, then each column in FP32) out. */
+int nsx_xpct_files(nsx_handle *h, const char *xvc_path, const char *out_prefix, int32_t precision);
+
 /* Lowest nev eigenpairs.  evals: host [nev]; evecs: host [nev][no_state] or NULL. */
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs,
               nsx_report *report);

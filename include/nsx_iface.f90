@@ -99,6 +99,20 @@ module nsx_iface
        type(c_ptr), value :: h
        type(nsx_plan_info), intent(out) :: info
      end function
+     integer(c_int) function nsx_expectation_matrix(h, vecs, nvec, precision, out) &
+          bind(C, name="nsx_expectation_matrix")
+       import :: c_int, c_ptr, c_int32_t, c_double
+       type(c_ptr), value :: h
+       real(c_double), dimension(*), intent(in) :: vecs
+       integer(c_int32_t), value :: nvec, precision
+       real(c_double), dimension(*), intent(out) :: out
+     end function
+     integer(c_int) function nsx_xpct_files(h, xvc_path, out_prefix, precision) bind(C, name="nsx_xpct_files")
+       import :: c_int, c_ptr, c_char, c_int32_t
+       type(c_ptr), value :: h
+       character(kind=c_char), dimension(*), intent(in) :: xvc_path, out_prefix   ! NUL-terminated
+       integer(c_int32_t), value :: precision
+     end function
      integer(c_int) function nsx_create(prob, device, out) bind(C, name="nsx_create")
        import :: c_int, c_ptr, nsx_problem
        type(nsx_problem), intent(in) :: prob

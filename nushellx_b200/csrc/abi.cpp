@@ -243,6 +243,26 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
   });
 }
 
+int nsx_expectation_matrix(nsx_handle *h, const double *vecs, int32_t nvec, int32_t precision, double *out) {
+  return guarded([&] {
+    if (!h || !vecs || !out) fail(NSX_E_ARG, "null argument");
+    require_device(h);
+    DeviceGuard dg(h->device);
+    expectation_matrix(h, vecs, nvec, precision, out);
+    check_device_error(h);
+  });
+}
+
+int nsx_xpct_files(nsx_handle *h, const char *xvc_path, const char *out_prefix, int32_t precision) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    require_device(h);
+    DeviceGuard dg(h->device);
+    xpct_files(h, xvc_path, out_prefix, precision);
+    check_device_error(h);
+  });
+}
+
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs, nsx_report *report) {
   return guarded([&] {
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");

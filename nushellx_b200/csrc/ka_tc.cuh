@@ -7,7 +7,7 @@
 //                                                           K = the slab's stacked rows.
 //
 // Operands: the Zbar tile (written by the mixing stage directly in the MN-major
-// 128-byte-swizzled layout, umma::a_sw128_index) and the slab's Abar (static, packed at
+// 128-byte / 32-byte-base swizzled layout, umma::a_sw128_index) and the slab's Abar (static, packed at
 // plan time K-major as umma::b_kmajor_index, split into its TF32 big and small parts)
 // stream through an S-stage shared-memory pipeline of bulk asynchronous copies, 32
 // stacked rows per stage.  After a stage lands, the 4 warps split Zbar into big/small
@@ -124,10 +124,10 @@ __global__ void __launch_bounds__(128, 1) k_a_tc(const ATileTC *__restrict__ til
       const uint32_t ar = umma::smem_u32(A_raw(s)), as = umma::smem_u32(A_sml(s));
       const uint32_t br = umma::smem_u32(B_big(s)), bs = umma::smem_u32(B_sml(s));
       for (int j = 0; j < ng; ++j) {
-        const uint64_t adb = umma::sdesc(ar + j * umma::A_GROUP_BYTES, umma::A_ATOM_BYTES, umma::A_GROUP_BYTES,
-                                         umma::LAYOUT_SW128);
-        const uint64_t ads = umma::sdesc(as + j * umma::A_GROUP_BYTES, umma::A_ATOM_BYTES, umma::A_GROUP_BYTES,
-                                         umma::LAYOUT_SW128);
+        const uint64_t adb = umma::sdesc(ar + j * umma::A_GROUP_BYTES, umma::A_ATOM_BYTES, umma::A_ROWS4_BYTES,
+                                         umma::LAYOUT_SW128_BASE32B);
+        const uint64_t ads = umma::sdesc(as + j * umma::A_GROUP_BYTES, umma::A_ATOM_BYTES, umma::A_ROWS4_BYTES,
+                                         umma::LAYOUT_SW128_BASE32B);
         const uint64_t bdb = umma::sdesc(br + j * NPAD * 32, NPAD * 16, 128, umma::LAYOUT_NONE);
         const uint64_t bds = umma::sdesc(bs + j * NPAD * 32, NPAD * 16, 128, umma::LAYOUT_NONE);
         umma::mma_tf32(tmem, adb, bdb, IDESC, (c > 0 || j > 0) ? 1u : 0u);

@@ -106,6 +106,8 @@ SYMBOLS = {
     "nsx_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "nsx_matvec_host": (C.c_int, [C.c_void_p, _p(C.c_double), _p(C.c_double), C.c_int32]),
     "nsx_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nsx_expectation_matrix": (C.c_int, [C.c_void_p, _p(C.c_double), C.c_int32, C.c_int32, _p(C.c_double)]),
+    "nsx_xpct_files": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int32]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
     "nsx_batch_solve": (C.c_int, [_p(C.c_void_p), C.c_int32, _p(Params), _p(_p(C.c_double)),
                                   _p(_p(C.c_double)), _p(Report)]),
@@ -324,6 +326,19 @@ class Solver:
         """FP64 H.v with the fixed device scratch array (no allocation in the call)."""
         _check(self._lib.nsx_matvec_noalloc(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                             C.c_void_p(stream) if stream else None))
+
+    def expectation_matrix(self, vecs, precision=NSX_FP64):
+        """matrixc(i, j) = (H v_i) . v_j for the rows of vecs (NuXpct's matrix; nsx_expectation_matrix)."""
+        v = np.ascontiguousarray(vecs, dtype=np.float64)
+        assert v.ndim == 2 and v.shape[1] == self.dim
+        out = np.zeros((v.shape[0], v.shape[0]), dtype=np.float64, order="F")
+        _check(self._lib.nsx_expectation_matrix(self._h, v.ctypes.data_as(_p(C.c_double)), v.shape[0], precision,
+                                                out.ctypes.data_as(_p(C.c_double))))
+        return out
+
+    def xpct_files(self, xvc_path, out_prefix, precision=NSX_FP64):
+        """NuXpct on files: .xvc in, <out_prefix>.ovl / .ovx out (nsx_xpct_files)."""
+        _check(self._lib.nsx_xpct_files(self._h, xvc_path.encode(), out_prefix.encode(), precision))
 
     def solve(self, nev=10, tol=1e-6, precision=NSX_FP64, window=100, keep=0, max_iter=3000, pre_iter=2,
               seed=5, start=None, refine=False, want_vectors=False):
