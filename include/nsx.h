@@ -206,6 +206,27 @@ int nsx_xpct_files(nsx_handle *h, const char *xvc_path, const char *out_prefix, 
 int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *evecs,
               nsx_report *report);
 
+/* The thick-restart state of a solve (the reference's TRL records: .abz matrix and counters,
+ * .trl basis vectors, src/NuLnz/NuCoreX.f90:266-292, 455-533): an orthonormal basis V, its
+ * projection T = V^T H V (tridiagonal with an arrowhead row after restarts) and the next
+ * Lanczos vector, with H V = V T + beta next e_m^T.  As output of nsx_solve_ex, m is the
+ * room of V and T in vectors on entry (window + 1 is always enough) and the vectors written
+ * on return; the state is the one at convergence. */
+typedef struct nsx_state {
+  int32_t m;                 /* basis vectors                                         */
+  double *V;                 /* [m][no_state] host                                    */
+  double *T;                 /* [m][m] column-major host                              */
+  double *next;              /* [no_state] host, unit norm                            */
+  double beta;               /* coupling of next to the last basis vector             */
+  int32_t iterations;        /* Lanczos steps made so far                             */
+  int32_t restarts;          /* thick restarts so far                                 */
+} nsx_state;
+/* nsx_solve, optionally resuming from a saved state (resume: the lowest params->keep Ritz
+ * vectors of its basis are kept, its next vector continues the recurrence; the start-vector
+ * fields of params are ignored) and optionally returning the final state (state_out). */
+int nsx_solve_ex(nsx_handle *h, const nsx_params *params, const nsx_state *resume, nsx_state *state_out,
+                 double *evals, double *evecs, nsx_report *report);
+
 /* Many independent solves at once (different J^pi, interaction variants or problems
  * of uneven size): problem i is nsx_solve(handles[i], &params[i], evals[i],
  * evecs ? evecs[i] : NULL, reports ? &reports[i] : NULL).  Every handle solves on its
@@ -230,6 +251,18 @@ int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *par
  * The reference names prefix Nucleus // file_code(J2/2, no_cA, no_cB). */
 int nsx_write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs,
                       int32_t nev, int32_t iterations, const char *intfile, int32_t T2);
+
+/* The thick-restart state in the reference's TRL files, as NuTRL leaves them at convergence
+ * (src/NuLnz/NuCoreX.f90:526-533, 280-281): <prefix>.abz with isave = state->m, alpha = diag T,
+ * betat = the subdiagonal, matrix = T, the counters, betat(isave+1) = beta; <prefix>.trl with the
+ * basis vectors and then the next vector (FP32 records); and, for the given eigenpairs, .lev
+ * and (evecs not NULL) .xvc.  NuVec's reconstruction from .abz/.trl gives the Ritz vectors. */
+int nsx_write_state(const nsx_handle *h, const char *prefix, const nsx_state *state, const double *evals,
+                    const double *evecs, int32_t nev, const char *intfile, int32_t T2);
+/* Reads <prefix>.abz / .trl written by nsx_write_state into a state for nsx_solve_ex's resume
+ * (the reference's TRL resume reads them at NuCoreX.f90:266-292); state->m is the room of
+ * state->V / state->T in vectors on entry. */
+int nsx_read_state(const nsx_handle *h, const char *prefix, nsx_state *state);
 
 /* Device-side statistics of a handle (for benchmarking and profiling).
  * Stages of one H.v: 0 = like-particle products (k_like), 1 = neutron-side Y

@@ -79,7 +79,40 @@ module nsx_iface
      integer(c_int64_t) :: tc_tiles(4), tc_chunks_max
   end type nsx_plan_info
 
+  type, bind(C) :: nsx_state
+     integer(c_int32_t) :: m
+     type(c_ptr)        :: V, T, next
+     real(c_double)     :: beta
+     integer(c_int32_t) :: iterations, restarts
+  end type nsx_state
+
   interface
+     integer(c_int) function nsx_solve_ex(h, params, resume, state_out, evals, evecs, report) &
+          bind(C, name="nsx_solve_ex")
+       import :: c_int, c_ptr, nsx_params, nsx_report
+       type(c_ptr), value :: h
+       type(nsx_params), intent(in) :: params
+       type(c_ptr), value :: resume, state_out     ! nsx_state or c_null_ptr
+       real(c_double), dimension(*), intent(out) :: evals
+       type(c_ptr), value :: evecs
+       type(nsx_report), intent(out) :: report
+     end function
+     integer(c_int) function nsx_write_state(h, prefix, state, evals, evecs, nev, intfile, T2) &
+          bind(C, name="nsx_write_state")
+       import :: c_int, c_ptr, c_char, c_int32_t, c_double, nsx_state
+       type(c_ptr), value :: h
+       character(kind=c_char), dimension(*), intent(in) :: prefix, intfile
+       type(nsx_state), intent(in) :: state
+       real(c_double), dimension(*), intent(in) :: evals
+       type(c_ptr), value :: evecs
+       integer(c_int32_t), value :: nev, T2
+     end function
+     integer(c_int) function nsx_read_state(h, prefix, state) bind(C, name="nsx_read_state")
+       import :: c_int, c_ptr, c_char, nsx_state
+       type(c_ptr), value :: h
+       character(kind=c_char), dimension(*), intent(in) :: prefix
+       type(nsx_state), intent(inout) :: state
+     end function
      integer(c_int) function nsx_create_z(prob, dop, device, out) bind(C, name="nsx_create_z")
        import :: c_int, c_ptr, nsx_problem, nsx_dop
        type(nsx_problem), intent(in) :: prob

@@ -19,7 +19,8 @@ void check_cuda(cudaError_t e, const char *what) {
   int code = (e == cudaErrorMemoryAllocation) ? NSX_E_NOMEM : NSX_E_CUDA;
   throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
 }
-void solve(nsx_handle *h, const nsx_params *P, double *evals, double *evecs, nsx_report *rep);
+void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_state *state_out, double *evals,
+           double *evecs, nsx_report *rep);
 std::shared_ptr<void> load_files(const nsx_files *f, nsx_problem *p);
 std::shared_ptr<void> compress_problem(const nsx_problem *p, const nsx_dop *d, nsx_problem *out);
 std::shared_ptr<DopArrays> read_dop(const std::string &path);
@@ -164,7 +165,8 @@ int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *par
       for (int i = next++; i < n; i = next++) {
         codes[i] = guarded([&] {
           NSX_CUDA(cudaSetDevice(handles[i]->device));
-          solve(handles[i], &params[i], evals[i], evecs ? evecs[i] : nullptr, reports ? &reports[i] : nullptr);
+          solve(handles[i], &params[i], nullptr, nullptr, evals[i], evecs ? evecs[i] : nullptr,
+                reports ? &reports[i] : nullptr);
         });
         if (codes[i] != NSX_OK) msgs[i] = g_err;
       }
@@ -183,6 +185,21 @@ int nsx_write_results(const nsx_handle *h, const char *prefix, const double *eva
   return guarded([&] {
     if (!h) fail(NSX_E_ARG, "null handle");
     write_results(h, prefix, evals, evecs, nev, iterations, intfile, T2);
+  });
+}
+
+int nsx_write_state(const nsx_handle *h, const char *prefix, const nsx_state *state, const double *evals,
+                    const double *evecs, int32_t nev, const char *intfile, int32_t T2) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    write_state(h, prefix, state, evals, evecs, nev, intfile, T2);
+  });
+}
+
+int nsx_read_state(const nsx_handle *h, const char *prefix, nsx_state *state) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    read_state(h, prefix, state);
   });
 }
 
@@ -268,7 +285,18 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
     require_device(h);
     DeviceGuard dg(h->device);
-    solve(h, params, evals, evecs, report);
+    solve(h, params, nullptr, nullptr, evals, evecs, report);
+    check_device_error(h);
+  });
+}
+
+int nsx_solve_ex(nsx_handle *h, const nsx_params *params, const nsx_state *resume, nsx_state *state_out,
+                 double *evals, double *evecs, nsx_report *report) {
+  return guarded([&] {
+    if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
+    require_device(h);
+    DeviceGuard dg(h->device);
+    solve(h, params, resume, state_out, evals, evecs, report);
     check_device_error(h);
   });
 }

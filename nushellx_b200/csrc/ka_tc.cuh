@@ -13,10 +13,14 @@
 // stacked rows per stage.  After a stage lands, the 4 warps split Zbar into big/small
 // parts in shared memory; one thread issues 3 MMAs per 8 stacked rows (big*big +
 // big*small + small*big: FP32 accuracy with FP32 accumulation in TMEM) and commits them
-// to the stage's mbarrier, which frees the stage for the copy S chunks ahead.  The
-// epilogue reads the 128 x N accumulator from TMEM (lane = output column) and adds it to
-// the output block, which the like-particle stage wrote first.  Each output element of a
-// slab tile belongs to one CTA: no atomics.
+// to the stage's mbarrier, which frees the stage for the copy S chunks ahead.  Each stage
+// accumulates into one of two TMEM accumulators (128 x N, lane = output column), taken in
+// turn; once a stage's MMAs have completed the 4 warps add its accumulator to FP32 registers.
+// (The tensor core's own accumulation over thousands of stacked rows loses bits at every
+// step, an error that grows with K; summing 32-row partial products in registers keeps the
+// product at FP32 accuracy.)  The registers are added to the output block, which the
+// like-particle stage wrote first.  Each output element of a slab tile belongs to one CTA: no
+// atomics.
 #pragma once
 #include "umma.cuh"
 
@@ -43,7 +47,7 @@ struct KaTcCfg {
   // + 1 KB alignment slack and a 16 KB tail that no copy writes: descriptor reads stay inside
   // the CTA's allocation even for the largest strides a descriptor field can encode here
   static constexpr size_t SMEM = (size_t)S * STAGE + 1024 + 16384;
-  static constexpr uint32_t TCOLS = NPAD <= 32 ? 32 : 64;         // TMEM columns (power of 2)
+  static constexpr uint32_t TCOLS = NPAD <= 16 ? 32 : (NPAD <= 32 ? 64 : 128);   // 2 accumulators, power of 2
 };
 
 template <int NPAD>
@@ -93,13 +97,31 @@ __global__ void __launch_bounds__(128, 1) k_a_tc(const ATileTC *__restrict__ til
     for (int c = 0; c < S && c < nchunk; ++c) issue(c);
 
   constexpr uint32_t IDESC = umma::idesc_tf32(NPAD, true);
-  bool bad0 = false;   // thread 0's own failed waits
+  const int m = warp * 32 + lane;   // output column within the tile = TMEM lane
+  float acc[NPAD];
+#pragma unroll
+  for (int i = 0; i < NPAD; ++i) acc[i] = 0.f;
+  // adds chunk cc's accumulator (columns (cc & 1) * NPAD ..) to the registers, once its MMAs completed
+  auto drain = [&](int cc) -> bool {
+    if (!umma::mbar_wait(&done[cc % S], (uint32_t)(cc / S) & 1u)) return false;
+    umma::tc_fence_after();
+#pragma unroll
+    for (int q = 0; q < NPAD / 16; ++q) {
+      float v[16];
+      umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((cc & 1) * NPAD + q * 16), v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[q * 16 + i] += v[i];
+    }
+    umma::tc_fence_before();
+    return true;
+  };
+  bool bad = false;   // this thread's failed waits
   int c = 0;
   bool ok = true;
   for (; c < nchunk; ++c) {
     const int s = c % S;
     const bool w = umma::mbar_wait(&full[s], (uint32_t)(c / S) & 1u);
-    if (__syncthreads_or(!w || bad0)) {
+    if (__syncthreads_or(!w || bad)) {
       ok = false;
       break;
     }
@@ -123,6 +145,7 @@ __global__ void __launch_bounds__(128, 1) k_a_tc(const ATileTC *__restrict__ til
       umma::tc_fence_after();
       const uint32_t ar = umma::smem_u32(A_raw(s)), as = umma::smem_u32(A_sml(s));
       const uint32_t br = umma::smem_u32(B_big(s)), bs = umma::smem_u32(B_sml(s));
+      const uint32_t dacc = tmem + (uint32_t)((c & 1) * NPAD);
       for (int j = 0; j < ng; ++j) {
         const uint64_t adb = umma::sdesc(ar + j * umma::A_GROUP_BYTES, umma::A_ATOM_BYTES, umma::A_ROWS4_BYTES,
                                          umma::LAYOUT_SW128_BASE32B);
@@ -130,37 +153,34 @@ __global__ void __launch_bounds__(128, 1) k_a_tc(const ATileTC *__restrict__ til
                                          umma::LAYOUT_SW128_BASE32B);
         const uint64_t bdb = umma::sdesc(br + j * NPAD * 32, NPAD * 16, 128, umma::LAYOUT_NONE);
         const uint64_t bds = umma::sdesc(bs + j * NPAD * 32, NPAD * 16, 128, umma::LAYOUT_NONE);
-        umma::mma_tf32(tmem, adb, bdb, IDESC, (c > 0 || j > 0) ? 1u : 0u);
-        umma::mma_tf32(tmem, adb, bds, IDESC, 1u);
-        umma::mma_tf32(tmem, ads, bdb, IDESC, 1u);
+        umma::mma_tf32(dacc, adb, bdb, IDESC, j > 0 ? 1u : 0u);   // a fresh partial sum per chunk
+        umma::mma_tf32(dacc, adb, bds, IDESC, 1u);
+        umma::mma_tf32(dacc, ads, bdb, IDESC, 1u);
       }
       umma::mma_commit(&done[s]);
-      // the stage of chunk c-1 is free once its MMAs have completed: refill it S chunks ahead
-      if (c >= 1 && c - 1 + S < nchunk) {
-        if (umma::mbar_wait(&done[(c - 1) % S], (uint32_t)((c - 1) / S) & 1u)) issue(c - 1 + S);
-        else bad0 = true;
-      }
+    }
+    // the previous chunk's partial sum: into the registers; its stage is then free for the
+    // copy S chunks ahead, and its accumulator for the chunk after this one
+    if (c >= 1) {
+      if (!drain(c - 1)) bad = true;
+      else if (tid == 0 && c - 1 + S < nchunk) issue(c - 1 + S);
     }
   }
-  // completion of every MMA issued (or of none), then the accumulator
+  if (ok && nchunk > 0 && !bad) {
+    if (!drain(nchunk - 1)) bad = true;
+  }
+  // completion of every MMA issued (or of none) before the accumulators are released
   if (tid == 0) {
     umma::mma_commit(&fin);
-    if (!umma::mbar_wait(&fin, 0)) bad0 = true;
+    if (!umma::mbar_wait(&fin, 0)) bad = true;
   }
-  if (__syncthreads_or(bad0)) ok = false;
+  if (__syncthreads_or(bad)) ok = false;
   if (ok) {
-    umma::tc_fence_after();
-    const int m = warp * 32 + lane;   // output column within the tile
-    float *o = out + t.out + (int64_t)t.ld * m;
+    if (m < t.ncols) {
+      float *o = out + t.out + (int64_t)t.ld * m;
 #pragma unroll
-    for (int q = 0; q < NPAD / 16; ++q) {
-      float v[16];
-      umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 16), v);
-      if (m < t.ncols) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (q * 16 + i < t.nl) o[q * 16 + i] += v[i];
-      }
+      for (int i = 0; i < NPAD; ++i)
+        if (i < t.nl) o[i] += acc[i];
     }
   } else if (tid == 0) {
     atomicOr(err, 1);

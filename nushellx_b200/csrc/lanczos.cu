@@ -556,7 +556,8 @@ struct Timer {
   }
 };
 
-void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_out, nsx_report *rep) {
+void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_state *state_out, double *evals_out,
+           double *evecs_out, nsx_report *rep) {
   auto t0 = std::chrono::steady_clock::now();
   const int64_t n = h->no_state;
   int64_t nallowed = 0;
@@ -588,18 +589,61 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   int matvecs = 0, iters = 0, restarts = 0;
   auto V = [&](int j) { return ws.V + (int64_t)j * n; };
 
+  std::vector<double> T((size_t)m * m, 0.0), theta, Sm;
+  std::vector<double> hcol(m + 2), h2(m + 2);
+  int i0 = 0, i = 0, nconv = 0;
+  if (resume) {
+    // a thick restart from a saved state (the reference's TRL resume, NuCoreX.f90:266-292): the
+    // lowest `keep` Ritz vectors of the saved basis, then the saved next vector
+    const int mr = resume->m;
+    if (mr < 1 || mr > m || !resume->V || !resume->T || !resume->next)
+      fail(NSX_E_ARG, "resume state: bad size (1.." + std::to_string(m) + " basis vectors) or null arrays");
+    NSX_CUDA(cudaMemcpyAsync(ws.V, resume->V, sizeof(double) * n * mr, cudaMemcpyHostToDevice, s));
+    std::vector<double> Tr(resume->T, resume->T + (size_t)mr * mr);
+    for (int c = 0; c < mr; ++c)
+      for (int r = 0; r < c; ++r) {
+        const double a = 0.5 * (Tr[r + (size_t)mr * c] + Tr[c + (size_t)mr * r]);
+        if (!std::isfinite(a)) fail(NSX_E_ARG, "resume state: T is not finite");
+        Tr[r + (size_t)mr * c] = Tr[c + (size_t)mr * r] = a;
+      }
+    jacobi(ws, mr, Tr, theta, Sm, s);
+    const int k = std::min(keep, mr);
+    std::vector<double> Sk((size_t)mr * k);
+    for (int c = 0; c < k; ++c)
+      for (int r = 0; r < mr; ++r) Sk[r + (size_t)mr * c] = Sm[r + (size_t)mr * c];
+    NSX_CUDA(cudaMemcpyAsync(ws.S, Sk.data(), sizeof(double) * Sk.size(), cudaMemcpyHostToDevice, s));
+    count_launch();
+    k_rotate<<<grid_for(n), 256, sizeof(double) * mr * k, s>>>(ws.V, n, mr, ws.S, k, ws.tmp, n);
+    NSX_CUDA(cudaMemcpyAsync(ws.V, ws.tmp, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
+    NSX_CUDA(cudaMemcpyAsync(ws.w, resume->next, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    cgs2(ws, k, ws.h, ws.h2, ws.h2 + k, s);   // the next vector, orthogonal to the kept ones
+    double nn2 = 0;
+    NSX_CUDA(cudaMemcpyAsync(&nn2, ws.h2 + k, sizeof(double), cudaMemcpyDeviceToHost, s));
+    NSX_CUDA(cudaStreamSynchronize(s));
+    if (!(nn2 > 1e-20) || !std::isfinite(nn2)) fail(NSX_E_ARG, "resume state: the next vector lies in the basis");
+    count_launch();
+    k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(k), ws.h2 + k, n);
+    NSX_CUDA(cudaGetLastError());
+    for (int c = 0; c < k; ++c) T[c + (size_t)m * c] = theta[c];
+    i0 = i = k;
+    iters = std::max(resume->iterations, 0);
+    restarts = std::max(resume->restarts, 0) + 1;
+  }
   // start vector
-  if (P->start) {
+  if (resume) {
+  } else if (P->start) {
     NSX_CUDA(cudaMemcpyAsync(V(0), P->start, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   } else {
     count_launch();
     k_rand<<<grid_for(n), 256, 0, s>>>(V(0), ws.mask, n, P->seed ? P->seed : 5);
   }
-  double nn = host_norm2(ws, V(0), n, s);
-  if (!(nn > 0) || !std::isfinite(nn)) fail(NSX_E_ARG, "start vector is zero or not finite");
-  count_launch();
-  k_scale<<<grid_for(n), 256, 0, s>>>(V(0), V(0), ws.h2, n);
-  for (int it = 0; it < P->pre_iter; ++it) {  // power pre-iterations (NuCoreX.f90:639-654)
+  if (!resume) {
+    double nn = host_norm2(ws, V(0), n, s);
+    if (!(nn > 0) || !std::isfinite(nn)) fail(NSX_E_ARG, "start vector is zero or not finite");
+    count_launch();
+    k_scale<<<grid_for(n), 256, 0, s>>>(V(0), V(0), ws.h2, n);
+  }
+  for (int it = 0; !resume && it < P->pre_iter; ++it) {  // power pre-iterations (NuCoreX.f90:639-654)
     tm.matvec(V(0), ws.w, prec, s);
     ++matvecs;
     dots(ws, ws.w, 0, 1, ws.w, n, ws.h2, false, s);
@@ -608,9 +652,6 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
   }
   NSX_CUDA(cudaGetLastError());
 
-  std::vector<double> T((size_t)m * m, 0.0), theta, Sm;
-  std::vector<double> hcol(m + 2), h2(m + 2);
-  int i0 = 0, i = 0, nconv = 0;
   std::vector<double> res(nev, 0.0);
   for (;;) {
     // ---- one Lanczos step on basis vector i: column i of T, v_{i+1} ----
@@ -679,6 +720,25 @@ void solve(nsx_handle *h, const nsx_params *P, double *evals_out, double *evecs_
       count_launch();
       k_rotate<<<grid_for(n), 256, smem, s>>>(ws.V, n, mm, ws.S, nev, ws.tmp, n);
       NSX_CUDA(cudaGetLastError());
+      if (state_out) {   // the basis, its projection and the next vector: H V = V T + beta next e_m^T
+        if (state_out->m < mm || !state_out->V || !state_out->T || !state_out->next)
+          fail(NSX_E_ARG, "state output: room for " + std::to_string(mm) + " basis vectors needed");
+        NSX_CUDA(cudaMemcpyAsync(state_out->V, ws.V, sizeof(double) * n * mm, cudaMemcpyDeviceToHost, s));
+        for (int c = 0; c < mm; ++c)
+          for (int r = 0; r < mm; ++r) state_out->T[r + (size_t)mm * c] = T[r + (size_t)m * c];
+        const bool scaled = !full && !exhausted;   // V(i+1) = w / beta was formed above
+        NSX_CUDA(cudaMemcpyAsync(state_out->next, scaled ? V(i + 1) : ws.w, sizeof(double) * n,
+                                 cudaMemcpyDeviceToHost, s));
+        NSX_CUDA(cudaStreamSynchronize(s));
+        if (!scaled) {
+          const double b = std::sqrt(std::max(h2[i + 1], 0.0));
+          for (int64_t e = 0; e < n; ++e) state_out->next[e] = b > 0 ? state_out->next[e] / b : 0.0;
+        }
+        state_out->m = mm;
+        state_out->beta = beta;
+        state_out->iterations = iters;
+        state_out->restarts = restarts;
+      }
       break;
     }
     if (!full) {

@@ -284,6 +284,9 @@ void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double 
 void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAGES], double flops[NSX_STAGES]);
 void flush_stage_events(nsx_handle *h);
 void check_device_error(nsx_handle *h);
+void write_state(const nsx_handle *h, const char *prefix, const nsx_state *st, const double *evals,
+                 const double *evecs, int nev, const char *intfile, int T2);
+void read_state(const nsx_handle *h, const char *prefix, nsx_state *st);
 void expectation_matrix(nsx_handle *h, const double *vecs, int nvec, int precision, double *out);
 void xpct_files(nsx_handle *h, const char *xvc_path, const char *out_prefix, int precision);
 void release_lanczos(nsx_handle *h);

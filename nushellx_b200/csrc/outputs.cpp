@@ -82,6 +82,40 @@ double positive_parity_share(const nsx_handle *h, const double *v) {
 }
 }  // namespace
 
+// NuVec's .xvc eigenvector file and the .lev level list for these eigenpairs.
+static void write_lev_xvc(const nsx_handle *h, const std::string &base, const double *evals, const double *evecs,
+                          int nev, const char *intfile, int T2) {
+  const int64_t n = h->no_state;
+  // .xvc
+  {
+    RecordWriter w(base + ".xvc");
+    w.put<int32_t>((int32_t)n);
+    w.put<int32_t>(nev);
+    w.end_record();
+    for (int i = 0; i < nev; ++i) {
+      w.put<float>((float)evals[i]);
+      const double *v = evecs + (size_t)i * n;
+      for (int64_t k = 0; k < n; ++k) w.put<float>((float)v[k]);
+      w.end_record();
+    }
+  }
+  // .lev
+  {
+    FILE *f = std::fopen((base + ".lev").c_str(), "w");
+    if (!f) fail(NSX_E_IO, "cannot write " + base + ".lev");
+    std::fprintf(f, "  %s\n\n", intfile ? intfile : "");
+    std::fprintf(f, "  2*J,   2*T %11d %11d\n\n", h->J2, T2);
+    std::fprintf(f, "  Lowest Energy Levels\n\n");
+    for (int i = 0; i < nev; ++i) {
+      const double share = positive_parity_share(h, evecs + (size_t)i * n);
+      const char par = share > 0.95 ? '+' : (share < 0.05 ? '-' : '?');
+      std::fprintf(f, "%10.3f%c", evals[i], par);
+      if (i % 5 == 4 || i == nev - 1) std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+  }
+}
+
 void write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs, int nev,
                    int iterations, const char *intfile, int T2) {
   if (!prefix || !evals || !evecs) fail(NSX_E_ARG, "null argument");
@@ -128,34 +162,123 @@ void write_results(const nsx_handle *h, const char *prefix, const double *evals,
     }
     std::fclose(f);
   }
-  // .xvc
+  write_lev_xvc(h, base, evals, evecs, nev, intfile, T2);
+}
+
+
+// The solver's thick-restart state as the reference's TRL leaves it (NuCoreX.f90:526-533 and the
+// .trl records): .abz with isave = m, alpha = diag T, betat = the subdiagonal, matrix = T, the
+// counters, and betat(isave+1) = beta; .trl with the m basis vectors and the next vector.  NuVec's
+// reconstruction (eigenvectors of the matrix times the records) gives the Ritz vectors; a resume
+// (read_state) continues from them.  .lev / .xvc carry the given eigenpairs (evecs may be null:
+// no .xvc then).
+void write_state(const nsx_handle *h, const char *prefix, const nsx_state *st, const double *evals,
+                 const double *evecs, int nev, const char *intfile, int T2) {
+  if (!prefix || !st || !evals || !st->V || !st->T || !st->next) fail(NSX_E_ARG, "null argument");
+  const int m = st->m;
+  if (m <= 0 || m + 1 > NOITER) fail(NSX_E_ARG, "state size out of range (1 .. 299)");
+  if (nev <= 0 || nev > m) fail(NSX_E_ARG, "nev out of range (1 .. state size)");
+  const std::string base(prefix);
+  const int64_t n = h->no_state;
   {
-    RecordWriter w(base + ".xvc");
-    w.put<int32_t>((int32_t)n);
-    w.put<int32_t>(nev);
+    RecordWriter w(base + ".abz");
+    w.put<int32_t>(m);
+    for (int i = 0; i < m; ++i) w.put<float>((float)st->T[i + (size_t)m * i]);
+    for (int i = 0; i < m; ++i) w.put<float>(i ? (float)st->T[i + (size_t)m * (i - 1)] : 0.f);
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) w.put<float>((float)st->T[i + (size_t)m * j]);
     w.end_record();
-    for (int i = 0; i < nev; ++i) {
-      w.put<float>((float)evals[i]);
-      const double *v = evecs + (size_t)i * n;
-      for (int64_t k = 0; k < n; ++k) w.put<float>((float)v[k]);
-      w.end_record();
+    const int32_t rec2[] = {st->iterations, nev};
+    w.put_bytes(rec2, sizeof(rec2));
+    w.put<float>(0.f);
+    const int32_t rec2b[] = {(int32_t)n, (int32_t)h->blocks.size(), 2, m, nev, FIRST_ITER_T, FIRST_ITER_T / 2, NOITER};
+    w.put_bytes(rec2b, sizeof(rec2b));
+    w.end_record();
+    for (const Block &b : h->blocks) {
+      unsigned char bas[8] = {(unsigned char)b.J2a, (unsigned char)b.J2b, 0, 0, 0, 0, 0, 0};
+      w.put_bytes(bas, 8);
     }
+    w.end_record();
+    for (int i = 0; i < NOITER; ++i) w.put<float>(i < nev ? (float)evals[i] : 0.f);
+    w.put<float>((float)st->beta);
+    for (int i = 0; i < NOITER; ++i) w.put<int32_t>(i < nev ? i + 1 : 0);
+    w.end_record();
   }
-  // .lev
   {
-    FILE *f = std::fopen((base + ".lev").c_str(), "w");
-    if (!f) fail(NSX_E_IO, "cannot write " + base + ".lev");
-    std::fprintf(f, "  %s\n\n", intfile ? intfile : "");
-    std::fprintf(f, "  2*J,   2*T %11d %11d\n\n", h->J2, T2);
-    std::fprintf(f, "  Lowest Energy Levels\n\n");
-    for (int i = 0; i < nev; ++i) {
-      const double share = positive_parity_share(h, evecs + (size_t)i * n);
-      const char par = share > 0.95 ? '+' : (share < 0.05 ? '-' : '?');
-      std::fprintf(f, "%10.3f%c", evals[i], par);
-      if (i % 5 == 4 || i == nev - 1) std::fprintf(f, "\n");
+    FILE *f = std::fopen((base + ".trl").c_str(), "wb");
+    if (!f) fail(NSX_E_IO, "cannot write " + base + ".trl");
+    std::vector<float> rec((size_t)n);
+    for (int i = 0; i <= m; ++i) {
+      const double *v = i < m ? st->V + (size_t)i * n : st->next;
+      for (int64_t k = 0; k < n; ++k) rec[k] = (float)v[k];
+      if (std::fwrite(rec.data(), 4, (size_t)n, f) != (size_t)n) {
+        std::fclose(f);
+        fail(NSX_E_IO, "write failed: " + base + ".trl");
+      }
     }
     std::fclose(f);
   }
+  if (evecs) write_lev_xvc(h, base, evals, evecs, nev, intfile, T2);
+}
+
+// The state written by write_state, for a resume (NuCoreX.f90:268-292 reads the same records).
+// st->m is the room of st->V / st->T in vectors on entry and the vectors read on return.
+void read_state(const nsx_handle *h, const char *prefix, nsx_state *st) {
+  if (!prefix || !st || !st->V || !st->T || !st->next) fail(NSX_E_ARG, "null argument");
+  const std::string base(prefix);
+  const int64_t n = h->no_state;
+  std::vector<std::vector<char>> recs;
+  {
+    FILE *f = std::fopen((base + ".abz").c_str(), "rb");
+    if (!f) fail(NSX_E_IO, "cannot open " + base + ".abz");
+    for (;;) {
+      uint32_t n1 = 0, n2 = 0;
+      if (std::fread(&n1, 4, 1, f) != 1) break;
+      std::vector<char> r(n1);
+      if ((n1 && std::fread(r.data(), 1, n1, f) != n1) || std::fread(&n2, 4, 1, f) != 1 || n1 != n2) {
+        std::fclose(f);
+        fail(NSX_E_IO, base + ".abz: truncated or inconsistent record");
+      }
+      recs.push_back(std::move(r));
+    }
+    std::fclose(f);
+  }
+  if (recs.size() < 4 || recs[0].size() < 4) fail(NSX_E_IO, base + ".abz: fewer than 4 records");
+  int32_t m;
+  std::memcpy(&m, recs[0].data(), 4);
+  if (m <= 0 || m + 1 > NOITER || recs[0].size() != 4 + 4 * (size_t)(2 * m + m * m))
+    fail(NSX_E_IO, base + ".abz: bad basis size in record 1");
+  if (m > st->m) fail(NSX_E_ARG, base + ": the state holds " + std::to_string(m) + " vectors, room for " +
+                                     std::to_string(st->m));
+  if (recs[1].size() < 12 || recs[3].size() < 4 * (size_t)(2 * NOITER + 1)) fail(NSX_E_IO, base + ".abz: short records");
+  int32_t imax, ns;
+  std::memcpy(&imax, recs[1].data(), 4);
+  std::memcpy(&ns, recs[1].data() + 12, 4);
+  if (ns != n) fail(NSX_E_ARG, base + ".abz: vector length differs from the handle's");
+  const char *mat = recs[0].data() + 4 + 8 * (size_t)m;
+  for (size_t e = 0; e < (size_t)m * m; ++e) {
+    float x;
+    std::memcpy(&x, mat + 4 * e, 4);
+    st->T[e] = x;
+  }
+  float b;
+  std::memcpy(&b, recs[3].data() + 4 * NOITER, 4);
+  FILE *f = std::fopen((base + ".trl").c_str(), "rb");
+  if (!f) fail(NSX_E_IO, "cannot open " + base + ".trl");
+  std::vector<float> rec((size_t)n);
+  for (int i = 0; i <= m; ++i) {
+    if (std::fread(rec.data(), 4, (size_t)n, f) != (size_t)n) {
+      std::fclose(f);
+      fail(NSX_E_IO, base + ".trl: fewer records than the .abz states");
+    }
+    double *v = i < m ? st->V + (size_t)i * n : st->next;
+    for (int64_t k = 0; k < n; ++k) v[k] = rec[k];
+  }
+  std::fclose(f);
+  st->m = m;
+  st->beta = b;
+  st->iterations = imax;
+  st->restarts = 0;
 }
 
 }  // namespace nsx

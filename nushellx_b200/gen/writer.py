@@ -193,9 +193,48 @@ def write_like(prefix_for_J, S, segs):
             w.write(i4(len(lst), S.dimJ(J2)), r4(X_STAMP))
 
 
-def write_problem(P, outdir, tag, no_level=10, dop_cut=None):
-    """Write all input files of problem P under outdir; returns the manifest dict.  With
-    dop_cut = (cut, cutm) also the compressed interaction <tag>i.dop of NuDiop (gen/dop.py)."""
+def _orbit_l(j2, parity):
+    """Orbital l of an orbit from 2j and its parity (-1)^l."""
+    lo = (j2 - 1) // 2
+    return lo if (1 if lo % 2 == 0 else -1) == parity else lo + 1
+
+
+def write_nus(path, P, nucleus):
+    """The model-space file NuLnz reads first (its reader: src/NuCommon/NuCommon.f90:2546-2736),
+    for the pn formalism: nucleus name, description, valence protons and neutrons, parity, the
+    shells (proton shells then neutron shells: number, n, l, 2j, 2t, parity), the 2J range (one
+    J here: the file is the per-J one that NuShellX's driver passes as NucleusJ), the 2T range
+    with nmp, the M-scheme truncation limits (none) and output control."""
+    sp = P.space
+    norb = sp.norb
+    lines = ["! model space of one J (written by the generator)", f"{nucleus:>6s}",
+             "synthetic interaction", "pn formalism", "one J", "! valence protons, neutrons",
+             f"{P.A.n} {P.B.n}", "! parity", f"{P.parity}", "! shells", f"{2 * norb}",
+             "p" * norb + "n" * norb]
+    for half in range(2):
+        for o in range(norb):
+            l = _orbit_l(sp.j2[o], sp.parity[o])
+            lines.append(f"{half * norb + o + 1} {0} {l} {sp.j2[o]} 1 {sp.parity[o]}")
+    tz2 = P.B.n - P.A.n
+    lines += ["! 2J range", f"{P.J2} {P.J2}", "! 2T range, nmp", f"{abs(tz2)} {P.A.n + P.B.n} {tz2}",
+              "! M-scheme truncation", "0 999",
+              " ".join(["0"] * (2 * norb)), " ".join(str(sp.j2[o % norb] + 1) for o in range(2 * norb)),
+              " ".join(["0"] * (2 * norb)), " ".join(str(sp.j2[o % norb] + 1) for o in range(2 * norb)),
+              "! output control", "1"]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+ANCODE = "0123456789_$cdefghijklmnopqrstuvwxyz@ABCDEFGHIJKLMNMPQRSTUVWXYZ"
+
+
+def write_problem(P, outdir, tag, no_level=10, dop_cut=None, restart=None):
+    """Write all input files of problem P under outdir; returns the manifest dict.  The names
+    follow NuShellX's command line for the Lanczos step (src/NuShellX/NuShellx.f90:1060-1061):
+    <tag><J code>.nus, <tag>a / <tag>b (.tri .trd and the like-particle .sgt/.mat), <tag>x
+    (.oph .spe); manifest["args"] is that command's five arguments.  With dop_cut = (cut, cutm)
+    also the compressed interaction <tag>x.dop of NuDiop (gen/dop.py); restart is the optional
+    fourth line of the .spe file."""
     os.makedirs(outdir, exist_ok=True)
     A, B = P.A, P.B
     norb = P.space.norb
@@ -204,22 +243,25 @@ def write_problem(P, outdir, tag, no_level=10, dop_cut=None):
     write_trd(base + "a.trd", A, P.rhoA, 2 * max(P.space.j2))
     write_tri(base + "b.tri", B, False)
     write_trd(base + "b.trd", B, P.rhoB, 2 * max(P.space.j2))
-    write_oph(base + "i.oph", P.vlam, norb, P.space.parity)
-    write_spe(base + "i.spe", P.space.spe, P.renorm, no_level)
+    write_oph(base + "x.oph", P.vlam, norb, P.space.parity)
+    write_spe(base + "x.spe", P.space.spe, P.renorm, no_level, restart)
+    nus = base + ANCODE[P.J2 // 2]
+    write_nus(nus + ".nus", P, tag[-6:])
     la = like_file_names(base + "a", A, -A.n, "x")
     lb = like_file_names(base + "b", B, B.n, "x")
     write_like(la, A, P.segA)
     write_like(lb, B, P.segB)
     man = {
-        "a": base + "a", "b": base + "b", "int": base + "i", "like_a": base + "a", "like_b": base + "b",
+        "a": base + "a", "b": base + "b", "int": base + "x", "like_a": base + "a", "like_b": base + "b",
+        "args": [nus, base + "a", base + "b", base + "x", tag], "nucleus": tag[-6:],
         "J2": P.J2, "parity": P.parity, "nprot": A.n, "nneut": B.n, "norb": norb,
         "shell_parity": list(P.space.parity) * 2,
         "no_state": P.no_state, "nblocks": len(P.blocks),
     }
     if dop_cut is not None:
         from .dop import diop, write_dop
-        write_dop(base + "i.dop", diop(P.vlam, P.space, *dop_cut))
-        man["dop"] = base + "i.dop"
+        write_dop(base + "x.dop", diop(P.vlam, P.space, *dop_cut))
+        man["dop"] = base + "x.dop"
     with open(base + ".json", "w") as f:
         json.dump(man, f, indent=1)
     return man

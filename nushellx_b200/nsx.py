@@ -73,6 +73,11 @@ class Files(C.Structure):
                 ("nshells", C.c_int32), ("nshells_p", C.c_int32), ("shell_parity", _p(C.c_int32))]
 
 
+class State(C.Structure):
+    _fields_ = [("m", C.c_int32), ("V", _p(C.c_double)), ("T", _p(C.c_double)), ("next", _p(C.c_double)),
+                ("beta", C.c_double), ("iterations", C.c_int32), ("restarts", C.c_int32)]
+
+
 class Dop(C.Structure):
     _fields_ = [("nterms", C.c_int32), ("lam2", _p(C.c_int32)), ("parity", _p(C.c_int32)), ("eig", _p(C.c_int32)),
                 ("e", _p(C.c_double)), ("shells", _p(C.c_uint8)), ("u", _p(C.c_double))]
@@ -108,6 +113,11 @@ SYMBOLS = {
     "nsx_matvec_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nsx_expectation_matrix": (C.c_int, [C.c_void_p, _p(C.c_double), C.c_int32, C.c_int32, _p(C.c_double)]),
     "nsx_xpct_files": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int32]),
+    "nsx_solve_ex": (C.c_int, [C.c_void_p, _p(Params), _p(State), _p(State), _p(C.c_double), _p(C.c_double),
+                               _p(Report)]),
+    "nsx_write_state": (C.c_int, [C.c_void_p, C.c_char_p, _p(State), _p(C.c_double), _p(C.c_double), C.c_int32,
+                                  C.c_char_p, C.c_int32]),
+    "nsx_read_state": (C.c_int, [C.c_void_p, C.c_char_p, _p(State)]),
     "nsx_solve": (C.c_int, [C.c_void_p, _p(Params), _p(C.c_double), _p(C.c_double), _p(Report)]),
     "nsx_batch_solve": (C.c_int, [_p(C.c_void_p), C.c_int32, _p(Params), _p(_p(C.c_double)),
                                   _p(_p(C.c_double)), _p(Report)]),
@@ -358,6 +368,72 @@ class Solver:
         out = rep.as_dict()
         out["residual"] = [rep.residual[i] for i in range(min(nev, 64))]
         return ev, vecs, out
+
+    def solve_state(self, nev=10, tol=1e-6, precision=NSX_FP64, window=100, keep=0, max_iter=3000, pre_iter=2,
+                    seed=5, start=None, refine=False, resume=None):
+        """nsx_solve_ex: a solve that returns its thick-restart state (dict V, T, next, beta,
+        iterations, restarts) and can resume from one.  Returns (evals, vecs, report, state)."""
+        p = Params()
+        p.nev, p.tol, p.precision, p.window, p.keep = nev, tol, precision, window, keep
+        p.max_iter, p.pre_iter, p.seed, p.refine = max_iter, pre_iter, seed, int(bool(refine))
+        st = None
+        if start is not None:
+            st = np.ascontiguousarray(start, dtype=np.float64)
+            p.start = st.ctypes.data_as(_p(C.c_double))
+        keep_alive = []
+        rs = None
+        if resume is not None:
+            V = np.ascontiguousarray(resume["V"], dtype=np.float64)
+            T = np.asfortranarray(resume["T"], dtype=np.float64)
+            nx = np.ascontiguousarray(resume["next"], dtype=np.float64)
+            keep_alive += [V, T, nx]
+            rs = State(V.shape[0], V.ctypes.data_as(_p(C.c_double)), T.ctypes.data_as(_p(C.c_double)),
+                       nx.ctypes.data_as(_p(C.c_double)), float(resume["beta"]), int(resume.get("iterations", 0)),
+                       int(resume.get("restarts", 0)))
+        cap = min(window, 112) + 1
+        Vo = np.zeros((cap, self.dim))
+        To = np.zeros(cap * cap)
+        No = np.zeros(self.dim)
+        so = State(cap, Vo.ctypes.data_as(_p(C.c_double)), To.ctypes.data_as(_p(C.c_double)),
+                   No.ctypes.data_as(_p(C.c_double)), 0.0, 0, 0)
+        ev = np.zeros(nev)
+        vecs = np.zeros((nev, self.dim))
+        rep = Report()
+        _check(self._lib.nsx_solve_ex(self._h, C.byref(p), C.byref(rs) if rs is not None else None, C.byref(so),
+                                      ev.ctypes.data_as(_p(C.c_double)), vecs.ctypes.data_as(_p(C.c_double)),
+                                      C.byref(rep)))
+        m = so.m
+        state = {"V": Vo[:m].copy(), "T": To[:m * m].reshape(m, m, order="F").copy(), "next": No, "beta": so.beta,
+                 "iterations": so.iterations, "restarts": so.restarts}
+        out = rep.as_dict()
+        out["residual"] = [rep.residual[i] for i in range(min(nev, 64))]
+        return ev, vecs, out, state
+
+    def write_state(self, prefix, state, evals, vecs=None, intfile="", T2=0):
+        """The reference's TRL files for a state (nsx_write_state): .abz/.trl, .lev, .xvc."""
+        V = np.ascontiguousarray(state["V"], dtype=np.float64)
+        T = np.asfortranarray(state["T"], dtype=np.float64)
+        nx = np.ascontiguousarray(state["next"], dtype=np.float64)
+        st = State(V.shape[0], V.ctypes.data_as(_p(C.c_double)), T.ctypes.data_as(_p(C.c_double)),
+                   nx.ctypes.data_as(_p(C.c_double)), float(state["beta"]), int(state["iterations"]),
+                   int(state["restarts"]))
+        ev = np.ascontiguousarray(evals, dtype=np.float64)
+        vv = np.ascontiguousarray(vecs, dtype=np.float64) if vecs is not None else None
+        _check(self._lib.nsx_write_state(self._h, prefix.encode(), C.byref(st), ev.ctypes.data_as(_p(C.c_double)),
+                                         vv.ctypes.data_as(_p(C.c_double)) if vv is not None else None, len(ev),
+                                         intfile.encode(), int(T2)))
+
+    def read_state(self, prefix, cap=113):
+        """A state written by write_state (nsx_read_state)."""
+        Vo = np.zeros((cap, self.dim))
+        To = np.zeros(cap * cap)
+        No = np.zeros(self.dim)
+        so = State(cap, Vo.ctypes.data_as(_p(C.c_double)), To.ctypes.data_as(_p(C.c_double)),
+                   No.ctypes.data_as(_p(C.c_double)), 0.0, 0, 0)
+        _check(self._lib.nsx_read_state(self._h, prefix.encode(), C.byref(so)))
+        m = so.m
+        return {"V": Vo[:m].copy(), "T": To[:m * m].reshape(m, m, order="F").copy(), "next": No, "beta": so.beta,
+                "iterations": so.iterations, "restarts": so.restarts}
 
     def write_results(self, prefix, evals, vecs, iterations=0, intfile="", T2=0):
         """The reference's .abz / .trl / .lev files for these eigenpairs (nsx_write_results)."""

@@ -87,7 +87,7 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
     from nushellx_b200 import nsx
     structs = {"nsx_species": nsx.Species, "nsx_problem": nsx.Problem, "nsx_params": nsx.Params,
                "nsx_report": nsx.Report, "nsx_files": nsx.Files, "nsx_stats": nsx.Stats,
-               "nsx_dop": nsx.Dop, "nsx_plan_info": nsx.PlanInfo}
+               "nsx_dop": nsx.Dop, "nsx_plan_info": nsx.PlanInfo, "nsx_state": nsx.State}
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "nsx.h"', 'int main(void) {']
     for cname, py in structs.items():
         src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
