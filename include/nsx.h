@@ -186,7 +186,8 @@ int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, voi
  * that loads the library until exit); larger problems are rejected with
  * NSX_E_ARG.  The first call on a device looks up the array's address: make it
  * before any stream capture.  All calls share the array; calls that overlap on
- * the GPU race.  x and y are DEVICE pointers; the operator data is the handle's. */
+ * the GPU race.  x and y are DEVICE pointers; the operator data is the handle's.  It never
+ * calls a shard's exchange: on a shard handle it writes the rank's rows only. */
 int nsx_matvec_noalloc(nsx_handle *h, const double *x, double *y, void *stream);
 
 /* The same with HOST pointers: copies in, multiplies, copies out, synchronises. */
@@ -297,6 +298,29 @@ typedef struct nsx_plan_info {
   int64_t tc_chunks_max;      /* most 32-row pipeline stages of one k_a_tc tile               */
 } nsx_plan_info;
 int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out);
+
+/* Output-block sharding of H.v over `world` GPUs, one process per GPU (the reference splits
+ * the same work over OpenMP threads by output block and J_ar, src/NuLnz/NuCoreX.f90:142-220).
+ * The blocks are cut into `world` contiguous ranges that minimise the largest range's flops;
+ * the handle of rank `rank` plans and computes the output rows of its range only, reading the
+ * whole input vector.  Without an exchange, its H.v writes rows [row_begin[rank],
+ * row_begin[rank+1]) of y and leaves the others as they were.  With an exchange (below),
+ * every product of the handle (nsx_matvec, nsx_solve, nsx_expectation_matrix, ...) ends with
+ * fn(user, y, no_state, stream): fn gets y with this rank's rows fresh and must fill the other
+ * ranks' rows (an all-gather, e.g. ncclAllGather over the ranks' communicator) before the work
+ * it enqueues on `stream` completes, and return 0.  Every rank then runs the same Lanczos
+ * recurrence on the whole vector.  Solves and expectation values on a handle with world > 1
+ * need an exchange.  world = 1 is the ordinary handle. */
+typedef int (*nsx_exchange_fn)(void *user, double *y, int64_t n, void *stream);
+int nsx_create_shard(const nsx_problem *prob, int device, int32_t rank, int32_t world, nsx_handle **out);
+int nsx_load_files_shard(const nsx_files *files, int device, int32_t rank, int32_t world, nsx_handle **out);
+/* rank, world, the rows of every rank (row_begin: world + 1 entries, may be null) and the
+ * flops of every rank's product as the split estimated them (world entries, may be null) */
+int nsx_shard_info(const nsx_handle *h, int32_t *rank, int32_t *world, int64_t *row_begin, double *est_flops);
+int nsx_set_exchange(nsx_handle *h, nsx_exchange_fn fn, void *user);
+/* The flops of every output block's rows (nsx_nblocks entries), the costs the split balances;
+ * a Y matrix read by several blocks counts for each of them. */
+int nsx_block_flops(const nsx_handle *h, double *out);
 
 /* Reset the counters; enable (1) or disable (0) per-stage event timing. */
 int nsx_stats_reset(nsx_handle *h, int32_t timing);

@@ -127,6 +127,41 @@ module nsx_iface
        integer(c_int), value :: device
        type(c_ptr), intent(out) :: out
      end function
+     ! output-block shards: rank's rows of H.v; the exchange (a bind(C) function
+     ! integer(c_int) fn(user, y, n, stream), e.g. an ncclAllGather) completes each product
+     integer(c_int) function nsx_create_shard(prob, device, rank, world, out) bind(C, name="nsx_create_shard")
+       import :: c_int, c_ptr, c_int32_t, nsx_problem
+       type(nsx_problem), intent(in) :: prob
+       integer(c_int), value :: device
+       integer(c_int32_t), value :: rank, world
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_load_files_shard(files, device, rank, world, out) &
+          bind(C, name="nsx_load_files_shard")
+       import :: c_int, c_ptr, c_int32_t, nsx_files
+       type(nsx_files), intent(in) :: files
+       integer(c_int), value :: device
+       integer(c_int32_t), value :: rank, world
+       type(c_ptr), intent(out) :: out
+     end function
+     integer(c_int) function nsx_shard_info(h, rank, world, row_begin, est_flops) bind(C, name="nsx_shard_info")
+       import :: c_int, c_ptr, c_int32_t, c_int64_t, c_double
+       type(c_ptr), value :: h
+       integer(c_int32_t), intent(out) :: rank, world
+       integer(c_int64_t), dimension(*), intent(out) :: row_begin   ! world + 1
+       real(c_double), dimension(*), intent(out) :: est_flops       ! world
+     end function
+     integer(c_int) function nsx_set_exchange(h, fn, user) bind(C, name="nsx_set_exchange")
+       import :: c_int, c_ptr, c_funptr
+       type(c_ptr), value :: h
+       type(c_funptr), value :: fn
+       type(c_ptr), value :: user
+     end function
+     integer(c_int) function nsx_block_flops(h, out) bind(C, name="nsx_block_flops")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), dimension(*), intent(out) :: out
+     end function
      integer(c_int) function nsx_get_plan_info(h, info) bind(C, name="nsx_get_plan_info")
        import :: c_int, c_ptr, nsx_plan_info
        type(c_ptr), value :: h

@@ -30,6 +30,12 @@ int noalloc_guarded(nsx_handle *h, const double *x, double *y, void *stream);
 static void require_device(const nsx_handle *h) {
   if (h->device < 0) fail(NSX_E_ARG, "the handle was created without a device (plan only)");
 }
+// Calls that need whole products (solves, expectation values): a shard needs its exchange.
+void require_full_product(const nsx_handle *h) {
+  if (h->shard_world > 1 && !h->exch)
+    fail(NSX_E_ARG, "the handle is one of " + std::to_string(h->shard_world) +
+                        " output-block shards: set an exchange (nsx_set_exchange) before solving");
+}
 
 template <typename F>
 static int guarded(F &&f) {
@@ -58,7 +64,8 @@ extern "C" {
 
 const char *nsx_last_error(void) { return g_err.c_str(); }
 
-int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
+// A handle for rank `rank` of `world` output-block shards (world = 1: the whole product).
+static int create_handle(const nsx_problem *prob, int device, int rank, int world, nsx_handle **out) {
   if (!out) {
     g_err = "null output handle pointer";
     return NSX_E_ARG;
@@ -71,13 +78,22 @@ int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
   }
   int rc = guarded([&] {
     if (!prob) fail(NSX_E_ARG, "null problem");
+    if (world < 1 || world > 1024) fail(NSX_E_ARG, "world size out of range (1 .. 1024)");
+    if (rank < 0 || rank >= world) fail(NSX_E_ARG, "rank out of range (0 .. world - 1)");
     h->device = device < 0 ? -1 : device;
-    if (device < 0) {   // plan only: no CUDA call at all
-      build_plan(h, prob);
-      return;
+    build_plan(h, prob);   // every block: the flops of each block's rows
+    if (world == 1) {
+      h->shard_first = {0, (int)h->blocks.size()};
+    } else {
+      h->shard_first = split_blocks(h->block_flops, world);
+      h->shard_rank = rank;
+      h->shard_world = world;
+      h->own_b0 = h->shard_first[rank];
+      h->own_b1 = h->shard_first[rank + 1];
+      build_plan(h, prob);   // this rank's blocks only
     }
+    if (device < 0) return;   // plan only: no CUDA call at all
     DeviceGuard dg(device);
-    build_plan(h, prob);
     upload(h);
   });
   if (rc != NSX_OK) {
@@ -89,7 +105,15 @@ int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
   return NSX_OK;
 }
 
-int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
+int nsx_create(const nsx_problem *prob, int device, nsx_handle **out) {
+  return create_handle(prob, device, 0, 1, out);
+}
+
+int nsx_create_shard(const nsx_problem *prob, int device, int32_t rank, int32_t world, nsx_handle **out) {
+  return create_handle(prob, device, rank, world, out);
+}
+
+int nsx_load_files_shard(const nsx_files *files, int device, int32_t rank, int32_t world, nsx_handle **out) {
   nsx_problem p;
   std::memset(&p, 0, sizeof(p));
   std::shared_ptr<void> store;
@@ -98,7 +122,44 @@ int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
     store = load_files(files, &p);
   });
   if (rc != NSX_OK) return rc;
-  return nsx_create(&p, device, out);
+  return create_handle(&p, device, rank, world, out);
+}
+
+int nsx_load_files(const nsx_files *files, int device, nsx_handle **out) {
+  return nsx_load_files_shard(files, device, 0, 1, out);
+}
+
+int nsx_shard_info(const nsx_handle *h, int32_t *rank, int32_t *world, int64_t *row_begin, double *est_flops) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    if (rank) *rank = h->shard_rank;
+    if (world) *world = h->shard_world;
+    const int nbl = (int)h->blocks.size();
+    for (int r = 0; r <= h->shard_world; ++r) {
+      const int b = h->shard_first[r];
+      if (row_begin) row_begin[r] = b < nbl ? h->blocks[b].off : h->no_state;
+      if (est_flops && r < h->shard_world) {
+        double f = 0.0;
+        for (int k = b; k < h->shard_first[r + 1]; ++k) f += h->block_flops[k];
+        est_flops[r] = f;
+      }
+    }
+  });
+}
+
+int nsx_block_flops(const nsx_handle *h, double *out) {
+  return guarded([&] {
+    if (!h || !out) fail(NSX_E_ARG, "null argument");
+    for (size_t i = 0; i < h->block_flops.size(); ++i) out[i] = h->block_flops[i];
+  });
+}
+
+int nsx_set_exchange(nsx_handle *h, nsx_exchange_fn fn, void *user) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    h->exch = fn;
+    h->exch_user = user;
+  });
 }
 
 int nsx_create_z(const nsx_problem *prob, const nsx_dop *dop, int device, nsx_handle **out) {
@@ -148,6 +209,7 @@ int nsx_batch_solve(nsx_handle *const *handles, int32_t n, const nsx_params *par
     for (int i = 0; i < n; ++i) {
       if (!hs[i] || !evals[i]) fail(NSX_E_ARG, "null handle or eigenvalue array for problem " + std::to_string(i));
       if (hs[i]->device < 0) fail(NSX_E_ARG, "problem " + std::to_string(i) + ": the handle was created without a device (plan only)");
+      require_full_product(hs[i]);
       for (int j = 0; j < i; ++j)
         if (hs[j] == hs[i]) fail(NSX_E_ARG, "the same handle is listed twice (problems " + std::to_string(j) +
                                                 " and " + std::to_string(i) + ")");
@@ -255,7 +317,12 @@ int nsx_matvec_host(nsx_handle *h, const double *x, double *y, int32_t precision
     size_t bytes = sizeof(double) * h->no_state;
     NSX_CUDA(cudaMemcpy(h->d.xin, x, bytes, cudaMemcpyHostToDevice));
     matvec_device(h, h->d.xin, h->d.xout, precision, 0);
-    NSX_CUDA(cudaMemcpy(y, h->d.xout, bytes, cudaMemcpyDeviceToHost));
+    if (h->shard_world > 1 && !h->exch) {   // this rank's rows only; the others stay as they were
+      NSX_CUDA(cudaMemcpy(y + h->row0, h->d.xout + h->row0, sizeof(double) * (h->row1 - h->row0),
+                          cudaMemcpyDeviceToHost));
+    } else {
+      NSX_CUDA(cudaMemcpy(y, h->d.xout, bytes, cudaMemcpyDeviceToHost));
+    }
     check_device_error(h);
   });
 }
@@ -264,6 +331,7 @@ int nsx_expectation_matrix(nsx_handle *h, const double *vecs, int32_t nvec, int3
   return guarded([&] {
     if (!h || !vecs || !out) fail(NSX_E_ARG, "null argument");
     require_device(h);
+    require_full_product(h);
     DeviceGuard dg(h->device);
     expectation_matrix(h, vecs, nvec, precision, out);
     check_device_error(h);
@@ -274,6 +342,7 @@ int nsx_xpct_files(nsx_handle *h, const char *xvc_path, const char *out_prefix, 
   return guarded([&] {
     if (!h) fail(NSX_E_ARG, "null handle");
     require_device(h);
+    require_full_product(h);
     DeviceGuard dg(h->device);
     xpct_files(h, xvc_path, out_prefix, precision);
     check_device_error(h);
@@ -284,6 +353,7 @@ int nsx_solve(nsx_handle *h, const nsx_params *params, double *evals, double *ev
   return guarded([&] {
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
     require_device(h);
+    require_full_product(h);
     DeviceGuard dg(h->device);
     solve(h, params, nullptr, nullptr, evals, evecs, report);
     check_device_error(h);
@@ -295,6 +365,7 @@ int nsx_solve_ex(nsx_handle *h, const nsx_params *params, const nsx_state *resum
   return guarded([&] {
     if (!h || !params || !evals) fail(NSX_E_ARG, "null argument");
     require_device(h);
+    require_full_product(h);
     DeviceGuard dg(h->device);
     solve(h, params, resume, state_out, evals, evecs, report);
     check_device_error(h);

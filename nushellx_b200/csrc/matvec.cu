@@ -934,12 +934,15 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
     run_stages<float>(h, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, nullptr, d.y32, d.z32, s);
-    {
+    if (h->row1 > h->row0) {   // the rows this handle computed (all of them unless it is a shard)
       StageScope sc(h, 4, s);
-      k_f2d<<<g, 256, 0, s>>>(d.o32, y, n);
+      k_f2d<<<g, 256, 0, s>>>(d.o32 + h->row0, y + h->row0, h->row1 - h->row0);
     }
     NSX_CUDA(cudaGetLastError());
   }
+  // a shard's product: the other ranks' rows come from the exchange
+  if (h->shard_world > 1 && h->exch && h->exch(h->exch_user, y, h->no_state, (void *)s) != 0)
+    fail(NSX_E_CUDA, "the exchange of the shards' rows failed");
 }
 
 // The FP64 stages with a caller-provided scratch buffer: Y (y_elems) and Zbar (z_elems) from

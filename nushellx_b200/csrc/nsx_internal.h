@@ -1,6 +1,7 @@
 // Internal structures of libnsx: host-side plan of one J-scheme pn problem and
 // the device buffers the H.v kernels and the Lanczos driver work on.
 #pragma once
+#include <climits>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -247,6 +248,15 @@ struct nsx_handle {
   int last_precision = NSX_FP64;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   void *lws = nullptr;   // the Lanczos solver's device workspace (lanczos.cu), kept between solves
+  // output-block shard: the plan covers the output rows of blocks [own_b0, own_b1), rows
+  // [row0, row1); shard_first[r] = first block of rank r (world + 1 entries)
+  int shard_rank = 0, shard_world = 1;
+  int own_b0 = 0, own_b1 = INT_MAX;
+  int64_t row0 = 0, row1 = 0;
+  std::vector<int> shard_first;
+  std::vector<double> block_flops;   // per output block: flops of its rows' product (estimate of the split)
+  nsx_exchange_fn exch = nullptr;
+  void *exch_user = nullptr;
 };
 
 namespace nsx {
@@ -272,6 +282,8 @@ struct DopArrays {
 // with 16-byte asynchronous copies).
 inline int64_t zbar_scratch_offset(const nsx_handle *h) { return (h->y_elems + 31) / 32 * 32; }
 void build_plan(nsx_handle *h, const nsx_problem *p);
+std::vector<int> split_blocks(const std::vector<double> &cost, int world);
+void require_full_product(const nsx_handle *h);
 void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
                      const double *b_seg_vals, int64_t b_nvals);
 void upload(nsx_handle *h);

@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <array>
 #include <map>
+#include <set>
 #include "nsx_internal.h"
 
 namespace nsx {
@@ -212,6 +214,16 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   }
   h->no_state = off;
   if (off == 0) fail(NSX_E_ARG, "empty J-scheme space");
+  // output-block shard: this handle plans the rows of blocks [own_b0, own_b1) only
+  const int nbl = (int)h->blocks.size();
+  const int ob0 = std::min(std::max(h->own_b0, 0), nbl), ob1 = std::min(std::max(h->own_b1, ob0), nbl);
+  auto owned = [&](int bl) { return bl >= ob0 && bl < ob1; };
+  h->row0 = ob0 < nbl ? h->blocks[ob0].off : off;
+  h->row1 = ob1 < nbl ? h->blocks[ob1].off : off;
+  // the flops of every block's rows come from the plan of the whole product (a shard's plan
+  // keeps those of the whole plan it was split from)
+  const bool whole = ob0 == 0 && ob1 == nbl;
+  if (whole) h->block_flops.assign(nbl, 0.0);
   std::map<std::pair<int, int>, int> bidx;
   for (size_t i = 0; i < h->blocks.size(); ++i) bidx[{h->blocks[i].J2a, h->blocks[i].J2b}] = (int)i;
   // parity mask lcoef (src/NuLnz/NuCoreX.f90:996-1030)
@@ -238,7 +250,8 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   // like-particle tiles and flops (segment count, src/NuCommonX/NuCommonX.f90:1009-1104)
   h->ltiles.clear();
   h->flops_like = 0;
-  for (auto &b : h->blocks) {
+  for (int bl = ob0; bl < ob1; ++bl) {
+    const Block &b = h->blocks[bl];
     if (b.da == 0 || b.db == 0) continue;
     for (int r0 = 0; r0 < b.da; r0 += 64)
       for (int c0 = 0; c0 < b.db; c0 += 64)
@@ -247,14 +260,20 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   for (int g = 0; g < p->a.nseg; ++g) {
     int J2s = p->a.seg_J2[g];
     double nn = (double)(p->a.seg_off[g + 1] - p->a.seg_off[g]) * (p->a.seg_np[g] == p->a.seg_npr[g] ? 1 : 2);
-    for (auto &b : h->blocks)
-      if (b.J2a == J2s) h->flops_like += 2.0 * nn * b.db;
+    for (int bl = 0; bl < nbl; ++bl)
+      if (h->blocks[bl].J2a == J2s) {
+        if (whole) h->block_flops[bl] += 2.0 * nn * h->blocks[bl].db;
+        if (owned(bl)) h->flops_like += 2.0 * nn * h->blocks[bl].db;
+      }
   }
   for (int g = 0; g < p->b.nseg; ++g) {
     int J2s = p->b.seg_J2[g];
     double nn = (double)(p->b.seg_off[g + 1] - p->b.seg_off[g]) * (p->b.seg_np[g] == p->b.seg_npr[g] ? 1 : 2);
-    for (auto &b : h->blocks)
-      if (b.J2b == J2s) h->flops_like += 2.0 * nn * b.da;
+    for (int bl = 0; bl < nbl; ++bl)
+      if (h->blocks[bl].J2b == J2s) {
+        if (whole) h->block_flops[bl] += 2.0 * nn * h->blocks[bl].da;
+        if (owned(bl)) h->flops_like += 2.0 * nn * h->blocks[bl].da;
+      }
   }
 
   // ---- pn table (drdbh, src/NuLnz/NuCoreX.f90:1428-1577) ----------------------
@@ -316,6 +335,28 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       nlayer[bk] = std::max(nlayer[bk], L + 1);
     }
   }
+  // Y flops of every output block's rows (for the shard split; the mixing and proton-side flops
+  // are added where the plan forms them), then the table keeps the owned blocks' rows only:
+  // every task list below follows from it.  A Y matrix counts for every block that reads it (a
+  // shard that owns two such blocks forms it once).
+  if (whole) {
+    std::vector<std::vector<double>> lnnz(B.keys.size());
+    for (size_t bk = 0; bk < B.keys.size(); ++bk) {
+      lnnz[bk].assign(nlayer[bk], 0.0);
+      const int J2bl = (int)(B.keys[bk] & 255), J2br = (int)((B.keys[bk] >> 8) & 255);
+      for (size_t bi = 0; bi < B.kblocks[bk].size(); ++bi) {
+        const RhoBlk &rb = B.kblocks[bk][bi];
+        lnnz[bk][blayer[bk][bi]] += (double)B.njt_of(rb.pl, J2bl) * B.njt_of(rb.pr, J2br);
+      }
+    }
+    std::set<std::array<int, 4>> yseen;   // (output block, input block, neutron key, layer)
+    for (const Row &r : table)
+      for (const Entry &e : r.e)
+        for (int L = 0; L < nlayer[e.bk]; ++L)
+          if (yseen.insert({r.bl, e.hb, e.bk, L}).second)
+            h->block_flops[r.bl] += 2.0 * h->blocks[e.hb].da * lnnz[e.bk][L];
+  }
+  table.erase(std::remove_if(table.begin(), table.end(), [&](const Row &r) { return !owned(r.bl); }), table.end());
   std::map<std::tuple<int, int, int>, int> ymat;
   std::vector<std::tuple<int, int, int>> ymats;
   std::vector<int64_t> yoff;
@@ -382,6 +423,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   // order; Abar = their density blocks side by side (nl x K column-major), Zbar = K x d_bl
   // row-major mixed operands written by k_z and consumed by k_a ----
   h->weights.clear();
+  h->wterms.clear();
   h->zgroups.clear();
   h->zsrcs.clear();
   h->zunits.clear();
@@ -466,6 +508,7 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           by_pr[rb.pr].push_back(op);
           h->flops_a += 2.0 * nl * nr * ob.db;
           h->flops_mix += 2.0 * nr * ob.db * G.ns;
+          if (whole) h->block_flops[bl] += 2.0 * nl * nr * ob.db + 2.0 * nr * ob.db * G.ns;
         }
       }
       for (auto &pp : by_pr)
@@ -615,6 +658,39 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
   for (auto &t : h->atiles) h->max_anl = std::max(h->max_anl, t.nl);
   h->max_zns = 0;
   for (auto &g : h->zgroups) h->max_zns = std::max(h->max_zns, g.ns);
+}
+
+// Contiguous split of the output blocks into `world` ranges that minimises the largest range's
+// flops (exact, by dynamic programming over the prefix sums).  first[r] = first block of rank r,
+// first[world] = the block count; ranks past the last block get empty ranges.
+std::vector<int> split_blocks(const std::vector<double> &cost, int world) {
+  const int n = (int)cost.size();
+  std::vector<double> S(n + 1, 0.0);
+  for (int i = 0; i < n; ++i) S[i + 1] = S[i] + cost[i];
+  const double INF = 1e300;
+  // best[k][i]: the smallest largest range when the first i blocks go to k ranks; cut[k][i] the
+  // start of the k-th range in that split
+  std::vector<std::vector<double>> best(world + 1, std::vector<double>(n + 1, INF));
+  std::vector<std::vector<int>> cut(world + 1, std::vector<int>(n + 1, 0));
+  best[0][0] = 0.0;
+  for (int k = 1; k <= world; ++k)
+    for (int i = 0; i <= n; ++i)
+      for (int j = 0; j <= i; ++j) {
+        if (best[k - 1][j] >= INF) continue;
+        const double v = std::max(best[k - 1][j], S[i] - S[j]);
+        if (v < best[k][i]) {   // strict: the earliest cut among equal splits
+          best[k][i] = v;
+          cut[k][i] = j;
+        }
+      }
+  std::vector<int> first(world + 1, n);
+  int i = n;
+  for (int k = world; k >= 1; --k) {
+    first[k] = i;
+    i = cut[k][i];
+  }
+  first[0] = 0;
+  return first;
 }
 
 }  // namespace nsx

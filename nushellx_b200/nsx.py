@@ -95,8 +95,16 @@ class PlanInfo(C.Structure):
         return d
 
 
+# int fn(void *user, double *y, int64_t n, void *stream): a shard's row exchange (nsx_set_exchange)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
+
 SYMBOLS = {
     "nsx_create": (C.c_int, [_p(Problem), C.c_int, _p(C.c_void_p)]),
+    "nsx_create_shard": (C.c_int, [_p(Problem), C.c_int, C.c_int32, C.c_int32, _p(C.c_void_p)]),
+    "nsx_load_files_shard": (C.c_int, [_p(Files), C.c_int, C.c_int32, C.c_int32, _p(C.c_void_p)]),
+    "nsx_shard_info": (C.c_int, [C.c_void_p, _p(C.c_int32), _p(C.c_int32), _p(C.c_int64), _p(C.c_double)]),
+    "nsx_set_exchange": (C.c_int, [C.c_void_p, EXCHANGE_FN, C.c_void_p]),
+    "nsx_block_flops": (C.c_int, [C.c_void_p, _p(C.c_double)]),
     "nsx_load_files": (C.c_int, [_p(Files), C.c_int, _p(C.c_void_p)]),
     "nsx_load_files_z": (C.c_int, [_p(Files), C.c_char_p, C.c_int, _p(C.c_void_p)]),
     "nsx_create_z": (C.c_int, [_p(Problem), _p(Dop), C.c_int, _p(C.c_void_p)]),
@@ -251,12 +259,16 @@ class Solver:
 
     # -- construction --------------------------------------------------------------
     @classmethod
-    def from_problem(cls, P, device=0):
-        """From an in-memory generated problem (FP64 operator data, no file rounding)."""
+    def from_problem(cls, P, device=0, shard=None):
+        """From an in-memory generated problem (FP64 operator data, no file rounding).  With
+        shard=(rank, world) the handle is rank's output-block shard (nsx_create_shard)."""
         lib = load_library()
         prob, keep = build_problem_struct(P)
         h = C.c_void_p()
-        _check(lib.nsx_create(C.byref(prob), device, C.byref(h)))
+        if shard is None:
+            _check(lib.nsx_create(C.byref(prob), device, C.byref(h)))
+        else:
+            _check(lib.nsx_create_shard(C.byref(prob), device, int(shard[0]), int(shard[1]), C.byref(h)))
         return cls(h, lib)
 
     @classmethod
@@ -283,10 +295,11 @@ class Solver:
         return cls(h, lib)
 
     @classmethod
-    def from_files(cls, manifest, device=0, dop=None):
+    def from_files(cls, manifest, device=0, dop=None, shard=None):
         """From the reference-format files described by a generator manifest (dict or .json path);
         with dop (a .dop path) the pn product uses NuTRLZ's compressed interaction
-        (nsx_load_files_z)."""
+        (nsx_load_files_z); with shard=(rank, world) the handle is rank's output-block shard
+        (nsx_load_files_shard)."""
         lib = load_library()
         if isinstance(manifest, str):
             with open(manifest) as f:
@@ -302,17 +315,24 @@ class Solver:
         f.nshells, f.nshells_p = 2 * m["norb"], m["norb"]
         f.shell_parity = sp.ctypes.data_as(_p(C.c_int32))
         h = C.c_void_p()
-        if dop is None:
+        if shard is not None:
+            if dop is not None:
+                raise ValueError("a shard handle takes the uncompressed interaction")
+            _check(lib.nsx_load_files_shard(C.byref(f), device, int(shard[0]), int(shard[1]), C.byref(h)))
+        elif dop is None:
             _check(lib.nsx_load_files(C.byref(f), device, C.byref(h)))
         else:
             _check(lib.nsx_load_files_z(C.byref(f), dop.encode(), device, C.byref(h)))
         return cls(h, lib)
 
     # -- operations -----------------------------------------------------------------
-    def matvec_host(self, x, precision=NSX_FP64):
+    def matvec_host(self, x, precision=NSX_FP64, out=None):
+        """H x with host arrays.  out: the result array (a shard handle without an exchange
+        writes its own rows of it and leaves the others)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         assert x.shape == (self.dim,)
-        y = np.empty_like(x)
+        y = np.empty_like(x) if out is None else out
+        assert y.dtype == np.float64 and y.shape == (self.dim,) and y.flags.c_contiguous
         _check(self._lib.nsx_matvec_host(self._h, x.ctypes.data_as(_p(C.c_double)),
                                          y.ctypes.data_as(_p(C.c_double)), precision))
         return y
@@ -468,6 +488,43 @@ class Solver:
             r["residual"] = [reps[i].residual[k] for k in range(min(nev, 64))]
             out.append((evs[i], vecs[i] if vecs else None, r))
         return out
+
+    def shard_info(self):
+        """{"rank", "world", "rows": first row of every rank (world + 1 entries), "est_flops"}."""
+        rank, world = C.c_int32(), C.c_int32()
+        _check(self._lib.nsx_shard_info(self._h, C.byref(rank), C.byref(world), None, None))
+        rows = np.zeros(world.value + 1, dtype=np.int64)
+        fl = np.zeros(world.value, dtype=np.float64)
+        _check(self._lib.nsx_shard_info(self._h, None, None, _ptr(rows, C.c_int64), _ptr(fl, C.c_double)))
+        return {"rank": rank.value, "world": world.value, "rows": rows, "est_flops": fl}
+
+    def block_flops(self):
+        """The flops of every output block's rows (what the shard split balances)."""
+        out = np.zeros(len(self.blocks), dtype=np.float64)
+        _check(self._lib.nsx_block_flops(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def set_exchange(self, fn):
+        """Every product of this shard handle ends with fn(y_ptr, n, stream_ptr), which must fill
+        the other ranks' rows of the device vector y (an all-gather) in the order of `stream`.
+        fn=None removes it.  An exception inside fn fails the product (NSX_E_CUDA) and is
+        kept in self.exchange_error."""
+        if fn is None:
+            self._exchange = None
+            _check(self._lib.nsx_set_exchange(self._h, EXCHANGE_FN(), None))
+            return
+        self.exchange_error = None
+
+        def cb(user, y, n, stream):
+            try:
+                fn(int(y or 0), int(n), int(stream or 0))
+                return 0
+            except BaseException as e:   # never let an exception cross the C frames
+                self.exchange_error = e
+                return 1
+
+        self._exchange = EXCHANGE_FN(cb)   # kept alive as long as the handle may call it
+        _check(self._lib.nsx_set_exchange(self._h, self._exchange, None))
 
     def stats_reset(self, timing=False):
         _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))

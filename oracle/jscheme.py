@@ -199,17 +199,24 @@ class Oracle:
         ja, jb = self.blocks[k]
         return x[self.off[k]:self.off[k + 1]].reshape(self.B.dim(jb), self.A.dim(ja)).T
 
-    def matvec(self, x):
+    def matvec(self, x, out_blocks=None):
+        """H x; with out_blocks (indices into self.blocks) only those output blocks' rows are
+        formed and the others are zero (one output-block shard's share)."""
         x = np.asarray(x, dtype=np.float64)
         y = np.zeros_like(x)
         A, B = self.A, self.B
+        own = set(range(len(self.blocks))) if out_blocks is None else set(out_blocks)
         for k, (ja, jb) in enumerate(self.blocks):
+            if k not in own:
+                continue
             C = self.block(x, k)
             if C.size == 0:
                 continue
             out = A.H[ja] @ C + C @ B.H[jb]
             y[self.off[k]:self.off[k + 1]] = out.T.ravel()
         for bl, ka, ents in self.table:
+            if bl not in own:
+                continue
             T = None
             for kb, hb, w in ents:
                 Ch = self.block(x, hb)
