@@ -51,7 +51,18 @@ METRIC = "time-to-10 eigenpairs @|dE|<1e-5 MeV: mixed+learned vs plain FP64, 1 B
 NEV = 10
 TOL = 1e-4        # Ritz residual tolerance of every timed or compared solve
 MODEL = os.path.join(ROOT, "nushellx_b200", "learned", "models", "fp_6p6n_0.npz")
-REF_ITERS = 300   # the reference's iteration cap noiter (src/NuCommonX/NuCommonX.f90:23-27)
+REF_ITERS = 300
+# the FP32 variants of the library's H.v (nsx_set_fp32_path); the library picks the fastest
+FP32_VARIANTS = {
+    1: "fp32 fused: neutron side formed inside the mixing stage (SIMT FP32, no Y in HBM), proton side on the "
+       "tensor cores (tcgen05.mma kind::tf32, 3xTF32 split, TMEM accumulators, bulk-copy pipeline); like-particle "
+       "part SIMT",
+    2: "fp32 tc: Y in HBM (k_y, mma.sync TF32 3xTF32), mixing into the tensor-core operand layout, proton side on "
+       "the tensor cores (tcgen05.mma kind::tf32, 3xTF32, TMEM accumulators); like-particle part SIMT",
+    3: "fp32 simt: Y in HBM (k_y, mma.sync TF32 3xTF32), SIMT mixing and proton side (cp.async pipeline); "
+       "like-particle part SIMT",
+}
+FP32_NAMES = {1: "fused", 2: "tc", 3: "simt"}   # the reference's iteration cap noiter (src/NuCommonX/NuCommonX.f90:23-27)
 
 
 def parse():
@@ -64,6 +75,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-hv", choices=["fp32", "fp64"], default=None)
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--fp32-path", choices=["auto", "fused", "tc", "simt", "all"], default="auto",
+                    help="with --profile-hv fp32: the FP32 variant (all: each in turn)")
     ap.add_argument("--ref-budget", type=float, default=600.0,
                     help="seconds of complete reference solves in the reference arm (at least one)")
     return ap.parse_args()
@@ -260,15 +273,27 @@ def run_profile_hv(args):
     S = Solver.from_problem(make_problem(args.workload))
     x = torch.randn(S.dim, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
-    S.matvec(x.data_ptr(), y.data_ptr(), prec)
-    torch.cuda.synchronize()
-    S.stats_reset(timing=True)
-    for _ in range(args.reps):
+    codes = {"auto": 0, "fused": 1, "tc": 2, "simt": 3}
+    if prec == NSX_FP64:
+        paths = [None]
+    elif args.fp32_path == "all":
+        paths = ([1] if S.plan_info()["fused_fp32"] else []) + [2, 3]
+    else:
+        paths = [codes[args.fp32_path]]
+    for p in paths:
+        if p is not None:
+            S.set_fp32_path(p)
         S.matvec(x.data_ptr(), y.data_ptr(), prec)
-    st = S.stats()["stages"]
-    per = {k: round(v["ms"] / v["launches"], 4) for k, v in st.items() if v["launches"]}
-    print(json.dumps({"workload": args.workload, "precision": args.profile_hv, "ms_per_launch": per,
-                      "max_abs_y": float(y.abs().max())}), flush=True)
+        torch.cuda.synchronize()
+        S.stats_reset(timing=True)
+        for _ in range(args.reps):
+            S.matvec(x.data_ptr(), y.data_ptr(), prec)
+        st = S.stats()["stages"]
+        per = {k: round(v["ms"] / v["launches"], 4) for k, v in st.items() if v["launches"]}
+        print(json.dumps({"workload": args.workload, "precision": args.profile_hv,
+                          "fp32_variant": FP32_NAMES.get(S.plan_info()["fp32_path"]) if p is not None else None,
+                          "ms_per_hv": per, "hv_ms": round(sum(per.values()), 4),
+                          "max_abs_y": float(y.abs().max())}), flush=True)
     S.close()
 
 
@@ -345,6 +370,7 @@ def run_ours(args, world, rank, local):
     for _ in range(10):
         S.matvec(x.data_ptr(), y.data_ptr(), NSX_FP32)
     st = S.stats()
+    fp32_path = S.plan_info()["fp32_path"]   # the variant the timed solves used
     S.stats_reset(timing=True)
     for _ in range(3):
         S.matvec(x.data_ptr(), y.data_ptr(), NSX_FP64)
@@ -372,6 +398,19 @@ def run_ours(args, world, rank, local):
         cmp["dE64"].append(float(np.abs(e64 - eref).max()))
     t_fp64 = max_over_ranks(float(np.mean(cmp["fp64_s"])), world)
     t_learned_same = max_over_ranks(float(np.mean(cmp["learned_s"])), world)
+    # every FP32 variant's stage times on the same vector (after all timed and compared solves)
+    variants_ms = {}
+    if rank == 0:
+        for p in ([1] if S.plan_info()["fused_fp32"] else []) + [2, 3]:
+            S.set_fp32_path(p)
+            S.matvec(x.data_ptr(), y.data_ptr(), NSX_FP32)
+            torch.cuda.synchronize()
+            S.stats_reset(timing=True)
+            for _ in range(5):
+                S.matvec(x.data_ptr(), y.data_ptr(), NSX_FP32)
+            sv = S.stats()["stages"]
+            variants_ms[FP32_NAMES[p]] = {k: round(v["ms"] / v["launches"], 4) for k, v in sv.items() if v["launches"]}
+        S.set_fp32_path(0)
     if rank != 0:
         S.close()
         return
@@ -414,9 +453,7 @@ def run_ours(args, world, rank, local):
                             else "standard (no model for this workload)",
                    "variants": f"TBME = base + sum_i lam_i P_i, lam ~ U[-0.3,0.3]^8 seed {vseed}, "
                                f"held-out indices {ntrain + args.warmup}..{ntrain + args.warmup + args.steps - 1}",
-                   "contraction": "fp32: proton side on the tensor cores (tcgen05.mma kind::tf32, 3xTF32 split, "
-                                  "TMEM accumulators, bulk-copy pipeline); neutron side fused into the mixing "
-                                  "stage (SIMT FP32, no Y in HBM); like-particle part SIMT",
+                   "contraction": FP32_VARIANTS.get(fp32_path, "unknown"),
                    "recurrence": "fp64", "window": 100,
                    "l2": "inputs larger than L2 (Zbar 2.0 GB, Lanczos basis 1.4 GB)",
                    "parallelism": "replicas" if world > 1 else "1 GPU"},
@@ -432,6 +469,7 @@ def run_ours(args, world, rank, local):
         "matvecs_per_s": float(sum(r["matvecs"] for r in reps)) / (ms / 1e3 * args.steps),
         "matvec_ms": {k: v["ms"] / max(v["launches"], 1) for k, v in stages.items() if v["launches"]},
         "matvec_ms_fp64": {k: v["ms"] / max(v["launches"], 1) for k, v in st64["stages"].items() if v["launches"]},
+        "fp32_variant": FP32_NAMES.get(fp32_path), "fp32_variants_ms_per_hv": variants_ms,
         "matvec_gflop": S.flops / 1e9,
         "matvec_tflop_per_s": S.flops / hv_s / 1e12, "matvec_fp64_tflop_per_s": S.flops / hv64_s / 1e12,
         "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": pk["tf"], "unit": "TFLOP/s",

@@ -290,14 +290,33 @@ typedef struct nsx_plan_info {
   int64_t zbar_tc_elems;      /* stacked operand elements, FP32 tensor-core tile layout       */
   int32_t y_row_tiles_max;    /* most 256-row tiles of one Y matrix (k_y)                     */
   int32_t group_sources_max;  /* most sources (h, b) of one mixing group                      */
-  int32_t fused_fp32;         /* 1: the FP32 form forms Y inside the mixing stage (k_yz)      */
+  int32_t fused_fp32;         /* 1: the fused FP32 variant (Y formed inside the mixing stage)
+                               *    is available (every mixing group has at most 16 sources)  */
   int32_t slab_rows_max;      /* longest stacked operand of an output slab                    */
   int32_t slab_splits_max;    /* most K pieces of one FP64 k_a slab tile (atomic partial sums) */
   int32_t slab_nl_max;        /* most rows of a proton partition (an output slab)             */
   int64_t tc_tiles[4];        /* k_a_tc tiles with N = 16, 32, 48, 64                         */
   int64_t tc_chunks_max;      /* most 32-row pipeline stages of one k_a_tc tile               */
+  int32_t fp32_path;          /* FP32 variant in use (NSX_FP32_*; 0 before the first FP32 H.v) */
+  int32_t pad;
 } nsx_plan_info;
 int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out);
+
+/* Variants of the FP32 product (no counterpart in the reference); all give the FP32 form's
+ * accuracy and differ in speed by problem:
+ *   NSX_FP32_FUSED  the neutron-side products formed inside the mixing stage (no Y in HBM,
+ *                   k_yz), the proton side on the tensor cores (k_a_tc, tcgen05);
+ *   NSX_FP32_TC     Y in HBM (k_y), mixing into the tensor-core operand layout (k_z), k_a_tc;
+ *   NSX_FP32_SIMT   k_y, k_z and the SIMT proton side (k_a).
+ * NSX_FP32_AUTO (the default) times the available variants on the handle's first FP32 product
+ * and keeps the fastest; that product synchronises its stream, so make it outside a stream
+ * capture (or choose a variant).  The buffers of the variants not kept are freed.  The fused
+ * variant needs every mixing group to have at most 16 sources (nsx_plan_info.fused_fp32). */
+#define NSX_FP32_AUTO 0
+#define NSX_FP32_FUSED 1
+#define NSX_FP32_TC 2
+#define NSX_FP32_SIMT 3
+int nsx_set_fp32_path(nsx_handle *h, int32_t path);
 
 /* Output-block sharding of H.v over `world` GPUs, one process per GPU (the reference splits
  * the same work over OpenMP threads by output block and J_ar, src/NuLnz/NuCoreX.f90:142-220).

@@ -77,6 +77,7 @@ module nsx_iface
      integer(c_int32_t) :: y_row_tiles_max, group_sources_max, fused_fp32
      integer(c_int32_t) :: slab_rows_max, slab_splits_max, slab_nl_max
      integer(c_int64_t) :: tc_tiles(4), tc_chunks_max
+     integer(c_int32_t) :: fp32_path, pad
   end type nsx_plan_info
 
   type, bind(C) :: nsx_state
@@ -161,6 +162,11 @@ module nsx_iface
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: h
        real(c_double), dimension(*), intent(out) :: out
+     end function
+     integer(c_int) function nsx_set_fp32_path(h, path) bind(C, name="nsx_set_fp32_path")
+       import :: c_int, c_ptr, c_int32_t
+       type(c_ptr), value :: h
+       integer(c_int32_t), value :: path   ! 0 auto, 1 fused, 2 tensor-core, 3 SIMT
      end function
      integer(c_int) function nsx_get_plan_info(h, info) bind(C, name="nsx_get_plan_info")
        import :: c_int, c_ptr, nsx_plan_info

@@ -414,7 +414,7 @@ int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out) {
     for (const auto &g : h->ygroups)
       out->y_row_tiles_max = std::max(out->y_row_tiles_max, (g.m + KY_TILE_ROWS - 1) / KY_TILE_ROWS);
     out->group_sources_max = h->max_zns;
-    out->fused_fp32 = h->max_zns <= 16 ? 1 : 0;
+    out->fused_fp32 = h->max_zns <= 16 ? 1 : 0;   // KYZ_NS
     std::map<std::pair<int64_t, int32_t>, int> pieces;   // (slab out offset, col0) -> K pieces
     for (const auto &t : h->atiles) {
       out->slab_rows_max = std::max(out->slab_rows_max, t.k_end);
@@ -423,6 +423,14 @@ int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out) {
     }
     for (int c = 0; c < 4; ++c) out->tc_tiles[c] = h->atc_off[c + 1] - h->atc_off[c];
     for (const auto &t : h->atiles_tc) out->tc_chunks_max = std::max<int64_t>(out->tc_chunks_max, (t.kgroups + 3) / 4);
+    out->fp32_path = h->fp32_path;
+  });
+}
+
+int nsx_set_fp32_path(nsx_handle *h, int32_t path) {
+  return guarded([&] {
+    if (!h) fail(NSX_E_ARG, "null handle");
+    set_fp32_path(h, path);
   });
 }
 

@@ -615,6 +615,31 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
     count_launch();
     k_rotate<<<grid_for(n), 256, sizeof(double) * mr * k, s>>>(ws.V, n, mr, ws.S, k, ws.tmp, n);
     NSX_CUDA(cudaMemcpyAsync(ws.V, ws.tmp, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
+    // A stored basis carries its storage's rounding (the reference's .trl records are FP32), so
+    // the rotated vectors are orthonormalised again in FP64 and their projection V_k^T H V_k is
+    // formed from k products instead of being taken as the stored matrix's Ritz values: the
+    // resumed recurrence then converges to the exact eigenvalues, not to those of the rounded
+    // state.
+    for (int j = 0; j < k; ++j) {
+      NSX_CUDA(cudaMemcpyAsync(ws.w, V(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      if (j == 0)
+        dots(ws, ws.w, 0, 1, ws.w, n, ws.h2, false, s);
+      else
+        cgs2(ws, j, ws.h, ws.h2, ws.h2 + j, s);
+      count_launch();
+      k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(j), ws.h2 + j, n);
+    }
+    for (int j = 0; j < k; ++j) {
+      tm.matvec(V(j), ws.w, prec, s);
+      ++matvecs;
+      dots(ws, ws.V, n, j + 1, ws.w, n, ws.h, false, s);
+      NSX_CUDA(cudaMemcpyAsync(hcol.data(), ws.h, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+      NSX_CUDA(cudaStreamSynchronize(s));
+      for (int r = 0; r <= j; ++r) {
+        if (!std::isfinite(hcol[r])) fail(NSX_E_NUMERIC, "non-finite projection of a resumed basis vector");
+        T[r + (size_t)m * j] = T[j + (size_t)m * r] = hcol[r];
+      }
+    }
     NSX_CUDA(cudaMemcpyAsync(ws.w, resume->next, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     cgs2(ws, k, ws.h, ws.h2, ws.h2 + k, s);   // the next vector, orthogonal to the kept ones
     double nn2 = 0;
@@ -624,7 +649,6 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
     count_launch();
     k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(k), ws.h2 + k, n);
     NSX_CUDA(cudaGetLastError());
-    for (int c = 0; c < k; ++c) T[c + (size_t)m * c] = theta[c];
     i0 = i = k;
     iters = std::max(resume->iterations, 0);
     restarts = std::max(resume->restarts, 0) + 1;

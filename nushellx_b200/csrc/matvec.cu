@@ -754,6 +754,7 @@ void upload(nsx_handle *h) {
   NSX_CUDA(cudaEventCreate(&h->ev1));
   // k_a's shared-memory cap: the same constant on every call (harmless to repeat)
   NSX_CUDA(cudaFuncSetAttribute(k_a<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<double>::bytes));
+  NSX_CUDA(cudaFuncSetAttribute(k_a<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaSmem<float>::bytes));
   NSX_CUDA(cudaFuncSetAttribute(k_a_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<16>::SMEM));
   NSX_CUDA(cudaFuncSetAttribute(k_a_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<32>::SMEM));
   NSX_CUDA(cudaFuncSetAttribute(k_a_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KaTcCfg<48>::SMEM));
@@ -774,17 +775,8 @@ void ensure_precision(nsx_handle *h, int precision) {
       NSX_CUDA(cudaMalloc(&d.z64, nz * sizeof(double)));
     }
   } else if (precision == NSX_FP32) {
-    if (!d.y32) {
-      // Zbar in the tensor-core tile layout; padding rows and columns stay zero for good.  The
-      // fused FP32 stage forms Y on chip: no Y buffer then.
-      const size_t nz32 = std::max<int64_t>(h->z32_elems, 1);
-      NSX_CUDA(cudaMalloc(&d.y32, (h->max_zns <= KYZ_NS ? 1 : ny) * sizeof(float)));
-      NSX_CUDA(cudaMalloc(&d.z32, nz32 * sizeof(float)));
-      NSX_CUDA(cudaMemset(d.z32, 0, nz32 * sizeof(float)));
-      d.abar_big = dev_copy_pod(h->abar_big);
-      d.abar_small = dev_copy_pod(h->abar_small);
-      d.zops_tc = dev_copy_pod(h->zops_tc);
-      d.atiles_tc = dev_copy_pod(h->atiles_tc);
+    if (!d.x32) {   // the data every FP32 variant reads; each variant's own buffers: ensure_fp32_path
+      (void)nz;
       d.rhoB32 = dev_copy<float>(h->yrho);
       d.hA32 = dev_copy<float>(h->A.hdense);
       d.hB32 = dev_copy<float>(h->B.hdense);
@@ -845,8 +837,10 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAG
   bytes[1] = es * (n + rhoB + y);                         // C in, rho_B, Y written
   bytes[2] = es * (y + z + (double)h->weights.size());    // Y in, Zbar written
   bytes[3] = es * (z + (double)h->abar.size() + 2.0 * n); // Zbar in, Abar, out read + written
-  const bool fused = precision == NSX_FP32 && h->max_zns <= KYZ_NS;
-  if (precision == NSX_FP32) {   // tensor-core layout of Zbar, split Abar
+  // the FP32 variant in use (before the first FP32 product: the fused one where it exists)
+  const int path = precision != NSX_FP32 ? 0 : (h->fp32_path ? h->fp32_path : (h->max_zns <= KYZ_NS ? 1 : 2));
+  const bool fused = path == NSX_FP32_FUSED;
+  if (path == NSX_FP32_FUSED || path == NSX_FP32_TC) {   // tensor-core layout of Zbar, split Abar
     bytes[2] = es * (y + (double)h->z32_elems + (double)h->weights.size());
     bytes[3] = es * ((double)h->z32_elems + 2.0 * (double)h->abar_big.size() + 2.0 * n);
   }
@@ -862,24 +856,66 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAG
   flops[4] = 0.0;
 }
 
+// The k_a_tc launches, one per N class, run concurrently: the class of 64-row partitions
+// (few tiles with the longest stacked operands) and the other non-empty classes start on
+// the handle's auxiliary streams, forked from and joined back into `s` with events, so that
+// the long tiles overlap the many short ones instead of following them.  Returns the launches.
+static int launch_ka_tc(nsx_handle *h, const float *Z, float *out, cudaStream_t s) {
+  auto &d = h->d;
+  int used[KTC_NCLASS], nu = 0;
+  for (int c = KTC_NCLASS - 1; c >= 0; --c)   // widest class first
+    if (h->atc_off[c + 1] > h->atc_off[c]) used[nu++] = c;
+  if (nu == 0) return 0;
+  if (nu > 1) {
+    if (!h->fork_ev) {
+      NSX_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+      for (int i = 0; i < KTC_NCLASS - 1; ++i) {
+        NSX_CUDA(cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
+        NSX_CUDA(cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
+      }
+    }
+    NSX_CUDA(cudaEventRecord(h->fork_ev, s));
+  }
+  for (int i = 0; i < nu; ++i) {
+    const int c = used[i];
+    cudaStream_t st = i + 1 < nu ? h->aux[i] : s;   // the last (narrowest) class on s itself
+    if (st != s) NSX_CUDA(cudaStreamWaitEvent(st, h->fork_ev, 0));
+    const unsigned n = (unsigned)(h->atc_off[c + 1] - h->atc_off[c]);
+    const ATileTC *tl = d.atiles_tc + h->atc_off[c];
+    switch (c) {
+      case 0: k_a_tc<16><<<n, 128, KaTcCfg<16>::SMEM, st>>>(tl, Z, d.abar_big, d.abar_small, out, d.err); break;
+      case 1: k_a_tc<32><<<n, 128, KaTcCfg<32>::SMEM, st>>>(tl, Z, d.abar_big, d.abar_small, out, d.err); break;
+      case 2: k_a_tc<48><<<n, 128, KaTcCfg<48>::SMEM, st>>>(tl, Z, d.abar_big, d.abar_small, out, d.err); break;
+      default: k_a_tc<64><<<n, 128, KaTcCfg<64>::SMEM, st>>>(tl, Z, d.abar_big, d.abar_small, out, d.err); break;
+    }
+    if (st != s) {
+      NSX_CUDA(cudaEventRecord(h->join_ev[i], st));
+      NSX_CUDA(cudaStreamWaitEvent(s, h->join_ev[i], 0));
+    }
+  }
+  NSX_CUDA(cudaGetLastError());
+  return nu;
+}
+
+// One product's stages.  path: 0 for FP64; for FP32 the variant (NSX_FP32_FUSED / _TC / _SIMT).
 template <typename T>
-static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoB, const T *hA, const T *hB, const T *w,
-                       const T *abar, T *Y, T *Z, cudaStream_t s) {
+static void run_stages(nsx_handle *h, int path, const T *x, T *out, const T *rhoB, const T *hA, const T *hB,
+                       const T *w, const T *abar, T *Y, T *Z, cudaStream_t s) {
   auto &d = h->d;
   if (!h->ltiles.empty()) {
     StageScope sc(h, 0, s);
     k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
   }
-  constexpr bool TC = std::is_same<T, float>::value;   // FP32: proton side on the tensor cores
-  const bool fused = TC && h->max_zns <= KYZ_NS;          // FP32: Y formed inside the mixing stage
+  constexpr bool F32 = std::is_same<T, float>::value;
+  const bool fused = F32 && path == NSX_FP32_FUSED;   // Y formed inside the mixing stage
+  const bool tc = F32 && path != NSX_FP32_SIMT;        // proton side on the tensor cores
   if (fused) {
-    if (!h->zunits.empty()) {
-      StageScope sc(h, 2, s);
-      k_yz<<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, d.yblks,
-                                                       reinterpret_cast<const float *>(w),
-                                                       reinterpret_cast<const float *>(x),
-                                                       reinterpret_cast<const float *>(rhoB),
-                                                       reinterpret_cast<float *>(Z));
+    if constexpr (F32) {
+      if (!h->zunits.empty()) {
+        StageScope sc(h, 2, s);
+        k_yz<<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, d.yblks, w, x,
+                                                         rhoB, Z);
+      }
     }
   } else {
     if (!h->ygroups.empty()) {
@@ -888,28 +924,26 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoB, const T
     }
     if (!h->zunits.empty()) {
       StageScope sc(h, 2, s);
+      const unsigned nu = (unsigned)h->zunits.size();
       // sources per group: registers for 16 unless the plan has a larger group
-      if (h->max_zns <= 16)
-        k_z<T, 16, TC><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc,
-                                                                   w, Y, Z);
-      else
-        k_z<T, ZMAXS, TC><<<(unsigned)h->zunits.size(), 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops,
-                                                                      d.zops_tc, w, Y, Z);
+      if (tc) {
+        if constexpr (F32) {
+          if (h->max_zns <= 16) k_z<T, 16, true><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+          else k_z<T, ZMAXS, true><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+        }
+      } else if (h->max_zns <= 16) {
+        k_z<T, 16, false><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+      } else {
+        k_z<T, ZMAXS, false><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+      }
     }
   }
-  if constexpr (TC) {
-    for (int c = 0; c < KTC_NCLASS; ++c) {
-      const int64_t n = h->atc_off[c + 1] - h->atc_off[c];
-      if (n == 0) continue;
-      StageScope sc(h, 3, s);
-      const ATileTC *tl = d.atiles_tc + h->atc_off[c];
-      float *o = reinterpret_cast<float *>(out);
-      const float *zf = reinterpret_cast<const float *>(Z);
-      switch (c) {
-        case 0: k_a_tc<16><<<(unsigned)n, 128, KaTcCfg<16>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
-        case 1: k_a_tc<32><<<(unsigned)n, 128, KaTcCfg<32>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
-        case 2: k_a_tc<48><<<(unsigned)n, 128, KaTcCfg<48>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
-        default: k_a_tc<64><<<(unsigned)n, 128, KaTcCfg<64>::SMEM, s>>>(tl, zf, d.abar_big, d.abar_small, o, d.err); break;
+  if (tc) {
+    if constexpr (F32) {
+      if (h->atc_off[KTC_NCLASS] > 0) {
+        StageScope sc(h, 3, s);   // one stage interval around the concurrent class launches
+        const int nl = launch_ka_tc(h, Z, out, s);
+        h->launches += nl - 1;
       }
     }
   } else if (!h->atiles.empty()) {
@@ -919,13 +953,127 @@ static void run_stages(nsx_handle *h, const T *x, T *out, const T *rhoB, const T
   NSX_CUDA(cudaGetLastError());
 }
 
+static bool fp32_path_available(const nsx_handle *h, int path) {
+  return path == NSX_FP32_TC || path == NSX_FP32_SIMT || (path == NSX_FP32_FUSED && h->max_zns <= KYZ_NS);
+}
+
+// The device buffers of one FP32 variant (allocated once; the tensor-core Zbar's padding rows
+// and columns stay zero for good).
+static void ensure_fp32_path(nsx_handle *h, int path) {
+  auto &d = h->d;
+  bool any = false;
+  if (path != NSX_FP32_FUSED && !d.y32) {
+    NSX_CUDA(cudaMalloc(&d.y32, std::max<int64_t>(h->y_elems, 1) * sizeof(float)));
+    any = true;
+  }
+  if (path != NSX_FP32_SIMT && !d.z32) {
+    const size_t nz32 = std::max<int64_t>(h->z32_elems, 1);
+    NSX_CUDA(cudaMalloc(&d.z32, nz32 * sizeof(float)));
+    NSX_CUDA(cudaMemset(d.z32, 0, nz32 * sizeof(float)));
+    d.abar_big = dev_copy_pod(h->abar_big);
+    d.abar_small = dev_copy_pod(h->abar_small);
+    d.zops_tc = dev_copy_pod(h->zops_tc);
+    d.atiles_tc = dev_copy_pod(h->atiles_tc);
+    any = true;
+  }
+  if (path == NSX_FP32_SIMT && !d.z32r) {
+    NSX_CUDA(cudaMalloc(&d.z32r, std::max<int64_t>(h->z_elems, 1) * sizeof(float)));
+    d.abar32 = dev_copy<float>(h->abar);
+    any = true;
+  }
+  if (any) NSX_CUDA(cudaDeviceSynchronize());   // copies from pageable memory have landed
+}
+
+// Frees what the chosen variant does not read.
+static void release_fp32_unused(nsx_handle *h, int path) {
+  auto &d = h->d;
+  auto drop = [](auto *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  };
+  if (path == NSX_FP32_FUSED) drop(d.y32);
+  if (path == NSX_FP32_SIMT) {
+    drop(d.z32);
+    drop(d.abar_big);
+    drop(d.abar_small);
+    drop(d.zops_tc);
+    drop(d.atiles_tc);
+  } else {
+    drop(d.z32r);
+    drop(d.abar32);
+  }
+}
+
+static void run_fp32(nsx_handle *h, int path, cudaStream_t s) {
+  auto &d = h->d;
+  run_stages<float>(h, path, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32, d.y32,
+                    path == NSX_FP32_SIMT ? d.z32r : d.z32, s);
+}
+
+// The variant of the handle's FP32 products: the requested one, or the fastest available one
+// timed on the product at hand (second of two runs each, CUDA events on `s`; the counters and
+// stage timings leave the trial runs out).
+static void choose_fp32_path(nsx_handle *h, cudaStream_t s) {
+  int best = h->fp32_request;
+  if (best == NSX_FP32_AUTO) {
+    const int64_t launches = h->launches;
+    int64_t sl[NSX_STAGES];
+    std::copy(h->stage_launches, h->stage_launches + NSX_STAGES, sl);
+    const bool timing = h->timing;
+    h->timing = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NSX_CUDA(cudaEventCreate(&e0));
+    NSX_CUDA(cudaEventCreate(&e1));
+    float tbest = 0.f;
+    try {
+      for (int p = NSX_FP32_FUSED; p <= NSX_FP32_SIMT; ++p) {
+        if (!fp32_path_available(h, p)) continue;
+        ensure_fp32_path(h, p);
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {
+          NSX_CUDA(cudaEventRecord(e0, s));
+          run_fp32(h, p, s);
+          NSX_CUDA(cudaEventRecord(e1, s));
+        }
+        NSX_CUDA(cudaEventSynchronize(e1));
+        NSX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (best == NSX_FP32_AUTO || ms < tbest) {
+          best = p;
+          tbest = ms;
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      h->timing = timing;
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->timing = timing;
+    h->launches = launches;
+    std::copy(sl, sl + NSX_STAGES, h->stage_launches);
+  }
+  ensure_fp32_path(h, best);
+  release_fp32_unused(h, best);
+  h->fp32_path = best;
+}
+
+void set_fp32_path(nsx_handle *h, int path) {
+  if (path < NSX_FP32_AUTO || path > NSX_FP32_SIMT) fail(NSX_E_ARG, "unknown FP32 variant");
+  if (path != NSX_FP32_AUTO && !fp32_path_available(h, path))
+    fail(NSX_E_ARG, "the fused FP32 variant needs mixing groups of at most 16 sources");
+  h->fp32_request = path;
+  h->fp32_path = 0;   // chosen again at the next FP32 product
+}
+
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s) {
   ensure_precision(h, precision);
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = precision;
   if (precision == NSX_FP64) {
-    run_stages<double>(h, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, d.y64, d.z64, s);
+    run_stages<double>(h, 0, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, d.y64, d.z64, s);
   } else {
     int64_t n = h->no_state;
     unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -933,7 +1081,8 @@ void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cud
       StageScope sc(h, 4, s);
       k_d2f<<<g, 256, 0, s>>>(x, d.x32, n);
     }
-    run_stages<float>(h, d.x32, d.o32, d.rhoB32, d.hA32, d.hB32, d.w32, nullptr, d.y32, d.z32, s);
+    if (h->fp32_path == 0) choose_fp32_path(h, s);
+    run_fp32(h, h->fp32_path, s);
     if (h->row1 > h->row0) {   // the rows this handle computed (all of them unless it is a shard)
       StageScope sc(h, 4, s);
       k_f2d<<<g, 256, 0, s>>>(d.o32 + h->row0, y + h->row0, h->row1 - h->row0);
@@ -951,7 +1100,7 @@ void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double 
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = NSX_FP64;
-  run_stages<double>(h, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
+  run_stages<double>(h, 0, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
 }
 
 // Fails with NSX_E_CUDA if a tensor-core kernel gave up a bounded wait since the last check
@@ -972,10 +1121,18 @@ void release(nsx_handle *h) {
   void *ptrs[] = {d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
                   d.abar_big, d.abar_small, d.zops_tc, d.atiles_tc, d.err,
                   d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zops, d.atiles, d.ltiles,
-                  d.y64, d.z64, d.y32, d.z32, d.x32, d.o32, d.xin, d.xout};
+                  d.y64, d.z64, d.y32, d.z32, d.z32r, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceBuffers();
+  for (int i = 0; i < KTC_NCLASS - 1; ++i) {
+    if (h->aux[i]) cudaStreamDestroy(h->aux[i]);
+    if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
+    h->aux[i] = nullptr;
+    h->join_ev[i] = nullptr;
+  }
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  h->fork_ev = nullptr;
   for (auto &e : h->stage_events) {
     cudaEventDestroy(e.second.first);
     cudaEventDestroy(e.second.second);

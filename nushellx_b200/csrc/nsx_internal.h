@@ -195,7 +195,8 @@ struct DeviceBuffers {
   ATile *atiles = nullptr;
   LTile *ltiles = nullptr;
   double *y64 = nullptr, *z64 = nullptr;  // Y and Zbar intermediates, FP64
-  float *y32 = nullptr, *z32 = nullptr;   // Y and Zbar intermediates, FP32
+  float *y32 = nullptr, *z32 = nullptr;   // Y and Zbar (tensor-core tile layout) intermediates, FP32
+  float *z32r = nullptr;                  // Zbar in the row-major layout of the SIMT proton side, FP32
   float *x32 = nullptr, *o32 = nullptr;
   double *xin = nullptr, *xout = nullptr;  // host-API staging
 };
@@ -248,6 +249,11 @@ struct nsx_handle {
   int last_precision = NSX_FP64;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   void *lws = nullptr;   // the Lanczos solver's device workspace (lanczos.cu), kept between solves
+  // FP32 variant (NSX_FP32_*): requested by nsx_set_fp32_path, and the one in use (0: not chosen)
+  int fp32_request = 0, fp32_path = 0;
+  // streams and events of the concurrent k_a_tc classes (created on first use)
+  cudaStream_t aux[nsx::KTC_NCLASS - 1] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[nsx::KTC_NCLASS - 1] = {};
   // output-block shard: the plan covers the output rows of blocks [own_b0, own_b1), rows
   // [row0, row1); shard_first[r] = first block of rank r (world + 1 entries)
   int shard_rank = 0, shard_world = 1;
@@ -290,6 +296,7 @@ void upload(nsx_handle *h);
 void upload_interaction(nsx_handle *h);
 cudaStream_t solve_stream(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
+void set_fp32_path(nsx_handle *h, int path);
 void release(nsx_handle *h);
 void matvec_device(nsx_handle *h, const double *x, double *y, int precision, cudaStream_t s);
 void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double *scratch, cudaStream_t s);

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libnsx.so")
 
 NSX_FP64 = 0
 NSX_FP32 = 1
+NSX_FP32_AUTO, NSX_FP32_FUSED, NSX_FP32_TC, NSX_FP32_SIMT = 0, 1, 2, 3
 _ERRNAMES = {-1: "NSX_E_ARG", -2: "NSX_E_IO", -3: "NSX_E_CUDA", -4: "NSX_E_NOMEM", -5: "NSX_E_NUMERIC",
              -6: "NSX_E_NOCONV"}
 
@@ -87,7 +88,8 @@ class PlanInfo(C.Structure):
     _fields_ = [("y_elems", C.c_int64), ("zbar_elems", C.c_int64), ("zbar_tc_elems", C.c_int64),
                 ("y_row_tiles_max", C.c_int32), ("group_sources_max", C.c_int32), ("fused_fp32", C.c_int32),
                 ("slab_rows_max", C.c_int32), ("slab_splits_max", C.c_int32), ("slab_nl_max", C.c_int32),
-                ("tc_tiles", C.c_int64 * 4), ("tc_chunks_max", C.c_int64)]
+                ("tc_tiles", C.c_int64 * 4), ("tc_chunks_max", C.c_int64), ("fp32_path", C.c_int32),
+                ("pad", C.c_int32)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "tc_tiles"}
@@ -132,6 +134,7 @@ SYMBOLS = {
     "nsx_write_results": (C.c_int, [C.c_void_p, C.c_char_p, _p(C.c_double), _p(C.c_double), C.c_int32, C.c_int32,
                                     C.c_char_p, C.c_int32]),
     "nsx_get_plan_info": (C.c_int, [C.c_void_p, _p(PlanInfo)]),
+    "nsx_set_fp32_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "nsx_stats_reset": (C.c_int, [C.c_void_p, C.c_int32]),
     "nsx_get_stats": (C.c_int, [C.c_void_p, _p(Stats)]),
     "nsx_destroy": (None, [C.c_void_p]),
@@ -528,6 +531,10 @@ class Solver:
 
     def stats_reset(self, timing=False):
         _check(self._lib.nsx_stats_reset(self._h, 1 if timing else 0))
+
+    def set_fp32_path(self, path):
+        """NSX_FP32_AUTO (0), NSX_FP32_FUSED (1), NSX_FP32_TC (2) or NSX_FP32_SIMT (3)."""
+        _check(self._lib.nsx_set_fp32_path(self._h, int(path)))
 
     def plan_info(self):
         """Which H.v kernel paths this handle's products take (nsx_get_plan_info)."""

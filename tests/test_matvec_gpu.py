@@ -26,6 +26,26 @@ def _rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+def _fp32_variants(S):
+    """The FP32 variants the handle can take (the fused one only with groups of <= 16 sources)."""
+    from nushellx_b200.nsx import NSX_FP32_FUSED, NSX_FP32_TC, NSX_FP32_SIMT
+    return ([NSX_FP32_FUSED] if S.plan_info()["fused_fp32"] else []) + [NSX_FP32_TC, NSX_FP32_SIMT]
+
+
+def check_fp32_variants(S, x, y_ref):
+    """Every FP32 variant against the oracle, then the automatic choice (one of them)."""
+    from nushellx_b200.nsx import NSX_FP32, NSX_FP32_AUTO
+    for p in _fp32_variants(S):
+        S.set_fp32_path(p)
+        y32 = S.matvec_host(x, NSX_FP32)
+        assert S.plan_info()["fp32_path"] == p
+        assert _rel(y32, y_ref) < FP32_TOL, (p, _rel(y32, y_ref))
+    S.set_fp32_path(NSX_FP32_AUTO)
+    y32 = S.matvec_host(x, NSX_FP32)
+    assert S.plan_info()["fp32_path"] in _fp32_variants(S)
+    assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
+
+
 @pytest.mark.parametrize("name", ["sd_2p2n_0", "sd_2p2n_2", "fp_4p4n_0"])
 def test_matvec_from_files_matches_oracle(name, files_dir):
     from oracle.jscheme import Oracle
@@ -42,8 +62,7 @@ def test_matvec_from_files_matches_oracle(name, files_dir):
         y_ref = O.matvec(x)
         y64 = S.matvec_host(x, NSX_FP64)
         assert _rel(y64, y_ref) < FP64_TOL, _rel(y64, y_ref)
-        y32 = S.matvec_host(x, NSX_FP32)
-        assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
+        check_fp32_variants(S, x, y_ref)
     S.close()
 
 
@@ -124,8 +143,11 @@ def test_matvec_benchmark_workload_matches_oracle(files_dir):
         y_ref = O.matvec(x)
         y64 = S.matvec_host(x, NSX_FP64)
         assert _rel(y64, y_ref) < FP64_TOL, _rel(y64, y_ref)
-        y32 = S.matvec_host(x, NSX_FP32)
-        assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
+        if trial == 0:
+            check_fp32_variants(S, x, y_ref)
+        else:
+            y32 = S.matvec_host(x, NSX_FP32)
+            assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
     S.close()
 
 
@@ -163,6 +185,5 @@ def test_matvec_kernel_paths_match_oracle(name, files_dir):
         y_ref = O.matvec(x)
         y64 = S.matvec_host(x, NSX_FP64)
         assert _rel(y64, y_ref) < FP64_TOL, _rel(y64, y_ref)
-        y32 = S.matvec_host(x, NSX_FP32)
-        assert _rel(y32, y_ref) < FP32_TOL, _rel(y32, y_ref)
+        check_fp32_variants(S, x, y_ref)
     S.close()

@@ -101,3 +101,24 @@ def test_plan_reaches_the_kernel_paths_the_gpu_tests_rely_on():
         S.close()
     info = Solver.from_problem(make_problem("fp_4p4n_0"), device=-1).plan_info()
     assert info["fused_fp32"] == 1 and info["slab_splits_max"] > 1
+
+
+def test_fp32_variant_requests_are_checked():
+    """nsx_set_fp32_path on plan-only handles: unknown variants and the fused variant on a plan
+    with a mixing group of more than 16 sources are refused; nothing is chosen before a product."""
+    from conftest import custom_problem
+    from nushellx_b200.nsx import Solver, NsxError, NSX_FP32_AUTO, NSX_FP32_FUSED, NSX_FP32_TC, NSX_FP32_SIMT
+    S = Solver.from_problem(make_problem("fp_4p4n_0"), device=-1)
+    for p in (NSX_FP32_AUTO, NSX_FP32_FUSED, NSX_FP32_TC, NSX_FP32_SIMT):
+        S.set_fp32_path(p)
+    for bad in (-1, 4):
+        with pytest.raises(NsxError):
+            S.set_fp32_path(bad)
+    assert S.plan_info()["fp32_path"] == 0
+    T = Solver.from_problem(custom_problem("FP", 5, 3, 2, 1, 5), device=-1)
+    assert T.plan_info()["fused_fp32"] == 0
+    with pytest.raises(NsxError, match="16 sources"):
+        T.set_fp32_path(NSX_FP32_FUSED)
+    T.set_fp32_path(NSX_FP32_TC)
+    S.close()
+    T.close()
