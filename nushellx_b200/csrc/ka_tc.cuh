@@ -40,18 +40,22 @@ constexpr int KTC_GROUPS = 4;   // 8-row groups per pipeline stage (32 stacked r
 
 template <int NPAD>
 struct KaTcCfg {
-  static constexpr int S = NPAD <= 32 ? 4 : 3;                    // pipeline stages
+  // pipeline stages; N = 16 (most tiles) takes 3 so that two CTAs share an SM
+  static constexpr int S = NPAD <= 16 ? 3 : (NPAD <= 32 ? 4 : 3);
+  static constexpr int MIN_CTAS = NPAD <= 16 ? 2 : 1;             // resident CTAs per SM
   static constexpr uint32_t A_BYTES = KTC_GROUPS * umma::A_GROUP_BYTES;  // 16 KB
   static constexpr uint32_t B_BYTES = KTC_GROUPS * NPAD * 32;     // one of big / small
   static constexpr uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  // + 1 KB alignment slack and a 16 KB tail that no copy writes: descriptor reads stay inside
-  // the CTA's allocation even for the largest strides a descriptor field can encode here
-  static constexpr size_t SMEM = (size_t)S * STAGE + 1024 + 16384;
+  // + 1 KB alignment slack and a 2 KB tail that no copy writes.  An MMA step reads exactly its
+  // operand footprint: A = 4 atoms (LBO 512 B apart) x 2 row groups (SBO 2048 B) = the 4096-byte
+  // group it starts, B = NPAD/8 core matrices (SBO 128 B) x 2 K halves (LBO NPAD*16 B) = its
+  // NPAD*32-byte group; the tail is margin beyond that.
+  static constexpr size_t SMEM = (size_t)S * STAGE + 1024 + 2048;
   static constexpr uint32_t TCOLS = NPAD <= 16 ? 32 : (NPAD <= 32 ? 64 : 128);   // 2 accumulators, power of 2
 };
 
 template <int NPAD>
-__global__ void __launch_bounds__(128, 1) k_a_tc(const ATileTC *__restrict__ tiles, const float *__restrict__ Zb,
+__global__ void __launch_bounds__(128, KaTcCfg<NPAD>::MIN_CTAS) k_a_tc(const ATileTC *__restrict__ tiles, const float *__restrict__ Zb,
                                                  const float *__restrict__ Bbig, const float *__restrict__ Bsml,
                                                  float *__restrict__ out, int *__restrict__ err) {
   using Cfg = KaTcCfg<NPAD>;

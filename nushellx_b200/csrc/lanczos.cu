@@ -103,13 +103,12 @@ __global__ void __launch_bounds__(256) k_sub(const double *__restrict__ V, int64
 }
 // ---- classical Gram-Schmidt with a second pass (CGS2) in three passes over the basis ----
 // Pass 1 (k_cg_dot):    h  = V^T w                         (V and w read once)
-// Pass 2 (k_cg_subdot): w -= V h, then h2 = V^T w          (V read once: each 64-row slice of
-//                        the basis is staged in shared memory and used for both products)
+// Pass 2 (k_cg_subdot): w -= V h, then h2 = V^T w          (V from HBM once: the second read
+//                        of each 128-row chunk of the basis is served from L2)
 // Pass 3 (k_cg_subnrm): w -= V h2, ||w||^2                 (V read once)
 // Per-CTA partial sums go to partial[cta][CG_MAXJ] and are added in a fixed order by
 // k_cg_reduce (deterministic).
 constexpr int CG_MAXJ = 128;   // basis vectors per pass (the window is capped below it)
-constexpr int CG_ROWS = 64;    // rows per staged slice of k_cg_subdot
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -117,77 +116,110 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Pass 1: each CTA takes row chunks of `chunk` rows (chunk <= CG_CHUNK_MAX; one chunk per CTA
+// when the vector allows), stages w's chunk in shared memory, and warp q forms the chunk's
+// dots with vectors q, q + 8, ..., reading each vector's chunk once with 32-lane coalesced
+// loads; the lanes' sums stay in registers until the CTA's last chunk.
 __global__ void __launch_bounds__(256) k_cg_dot(const double *__restrict__ V, int64_t ldv, int cnt,
-                                                const double *__restrict__ w, int64_t n, double *__restrict__ partial) {
-  __shared__ double acc[8][CG_MAXJ];
+                                                const double *__restrict__ w, int64_t n, int chunk,
+                                                double *__restrict__ partial) {
+  extern __shared__ double cg_sm[];   // [chunk]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int e = tid; e < 8 * CG_MAXJ; e += 256) (&acc[0][0])[e] = 0.0;
-  __syncthreads();
-  for (int64_t base = (int64_t)blockIdx.x * 1024; base < n; base += (int64_t)gridDim.x * 1024) {
-    double wv[4];
+  constexpr int JW = CG_MAXJ / 8;     // vectors per warp
+  double acc[JW];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t r = base + tid + 256 * k;
-      wv[k] = r < n ? w[r] : 0.0;
-    }
-    for (int j = 0; j < cnt; ++j) {
-      const double *vj = V + (int64_t)j * ldv;
-      double sj = 0.0;
+  for (int jj = 0; jj < JW; ++jj) acc[jj] = 0.0;
+  for (int64_t base = (int64_t)blockIdx.x * chunk; base < n; base += (int64_t)gridDim.x * chunk) {
+    const int rows = (int)(n - base < chunk ? n - base : chunk);
+    __syncthreads();
+    for (int r = tid; r < rows; r += 256) cg_sm[r] = w[base + r];
+    __syncthreads();
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int64_t r = base + tid + 256 * k;
-        if (r < n) sj = fma(vj[r], wv[k], sj);
+    for (int jj = 0; jj < JW; ++jj) {
+      const int j = warp + 8 * jj;
+      if (j < cnt) {
+        const double *vj = V + (int64_t)j * ldv + base;
+        double a0 = 0.0, a1 = 0.0;
+        int r = lane;
+        for (; r + 32 < rows; r += 64) {
+          a0 = fma(vj[r], cg_sm[r], a0);
+          a1 = fma(vj[r + 32], cg_sm[r + 32], a1);
+        }
+        if (r < rows) a0 = fma(vj[r], cg_sm[r], a0);
+        acc[jj] += a0 + a1;
       }
-      sj = warp_sum(sj);
-      if (lane == 0) acc[warp][j] += sj;
     }
   }
-  __syncthreads();
-  for (int j = tid; j < cnt; j += 256) {
-    double v = 0.0;
-    for (int q = 0; q < 8; ++q) v += acc[q][j];
-    partial[(int64_t)blockIdx.x * CG_MAXJ + j] = v;
+#pragma unroll
+  for (int jj = 0; jj < JW; ++jj) {
+    const int j = warp + 8 * jj;
+    const double v = warp_sum(acc[jj]);
+    if (lane == 0 && j < cnt) partial[(int64_t)blockIdx.x * CG_MAXJ + j] = v;
   }
 }
 
+// Pass 2 over row chunks of CG_SUB rows: w -= V h for the chunk (two threads per row, each
+// over half of the vectors), the chunk of w kept in shared memory, then warp q forms the
+// chunk's dots with vectors q, q + 8, ...  The second read of the chunk's basis rows follows
+// the first within the CTA, so it is served from L2 (the CTAs' chunks in flight together,
+// 592 x 128 rows x up to 128 vectors, fit in it): V crosses HBM once.
+constexpr int CG_SUB = 128;
 __global__ void __launch_bounds__(256) k_cg_subdot(const double *__restrict__ V, int64_t ldv, int cnt,
                                                    const double *__restrict__ h, double *__restrict__ w, int64_t n,
                                                    double *__restrict__ partial) {
-  extern __shared__ double cg_sm[];
-  double *Vs = cg_sm;                              // [cnt][CG_ROWS + 1]
-  double *hs = Vs + (size_t)cnt * (CG_ROWS + 1);   // [cnt]
-  double *ws = hs + CG_MAXJ;                       // [CG_ROWS]
-  const int tid = threadIdx.x;
+  __shared__ double hs[CG_MAXJ];
+  __shared__ double ws[CG_SUB];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int j = tid; j < cnt; j += 256) hs[j] = h[j];
-  double accj = 0.0;                               // thread j < cnt: the partial of h2[j]
-  for (int64_t base = (int64_t)blockIdx.x * CG_ROWS; base < n; base += (int64_t)gridDim.x * CG_ROWS) {
-    const int rows = (int)(n - base < CG_ROWS ? n - base : CG_ROWS);
-    __syncthreads();
-    for (int e = tid; e < cnt * CG_ROWS; e += 256) {
-      const int j = e / CG_ROWS, r = e - j * CG_ROWS;
-      Vs[j * (CG_ROWS + 1) + r] = r < rows ? V[(int64_t)j * ldv + base + r] : 0.0;
-    }
-    __syncthreads();
-    {  // w -= V h for the slice: 4 threads per row
-      const int row = tid >> 2, q = tid & 3;
-      double sv = 0.0;
-      for (int j = q; j < cnt; j += 4) sv = fma(Vs[j * (CG_ROWS + 1) + row], hs[j], sv);
+  constexpr int JW = CG_MAXJ / 8;
+  double acc[JW];
+#pragma unroll
+  for (int jj = 0; jj < JW; ++jj) acc[jj] = 0.0;
+  const int row = tid >> 1, half = tid & 1;
+  for (int64_t base = (int64_t)blockIdx.x * CG_SUB; base < n; base += (int64_t)gridDim.x * CG_SUB) {
+    const int rows = (int)(n - base < CG_SUB ? n - base : CG_SUB);
+    __syncthreads();   // hs loaded; the previous chunk's ws no longer read
+    {
+      double s0 = 0.0, s1 = 0.0;
+      if (row < rows) {
+        const double *vr = V + base + row;
+        int j = half;
+        for (; j + 2 < cnt; j += 4) {
+          s0 = fma(vr[(int64_t)j * ldv], hs[j], s0);
+          s1 = fma(vr[(int64_t)(j + 2) * ldv], hs[j + 2], s1);
+        }
+        if (j < cnt) s0 = fma(vr[(int64_t)j * ldv], hs[j], s0);
+      }
+      double sv = s0 + s1;
       sv += __shfl_xor_sync(0xffffffffu, sv, 1);
-      sv += __shfl_xor_sync(0xffffffffu, sv, 2);
-      if (q == 0) {
+      if (half == 0) {
         const double w1 = row < rows ? w[base + row] - sv : 0.0;
         ws[row] = w1;
         if (row < rows) w[base + row] = w1;
       }
     }
     __syncthreads();
-    if (tid < cnt) {
-      const double *vr = Vs + tid * (CG_ROWS + 1);
-#pragma unroll 8
-      for (int r = 0; r < CG_ROWS; ++r) accj = fma(vr[r], ws[r], accj);
+#pragma unroll
+    for (int jj = 0; jj < JW; ++jj) {
+      const int j = warp + 8 * jj;
+      if (j < cnt) {
+        const double *vj = V + (int64_t)j * ldv + base;
+        double a = 0.0;
+#pragma unroll
+        for (int q = 0; q < CG_SUB / 32; ++q) {
+          const int r = lane + 32 * q;
+          if (r < rows) a = fma(vj[r], ws[r], a);
+        }
+        acc[jj] += a;
+      }
     }
   }
-  if (tid < cnt) partial[(int64_t)blockIdx.x * CG_MAXJ + tid] = accj;
+#pragma unroll
+  for (int jj = 0; jj < JW; ++jj) {
+    const int j = warp + 8 * jj;
+    const double v = warp_sum(acc[jj]);
+    if (lane == 0 && j < cnt) partial[(int64_t)blockIdx.x * CG_MAXJ + j] = v;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_cg_subnrm(const double *__restrict__ V, int64_t ldv, int cnt,
@@ -200,8 +232,18 @@ __global__ void __launch_bounds__(256) k_cg_subnrm(const double *__restrict__ V,
   __syncthreads();
   double nrm = 0.0;
   for (int64_t r = (int64_t)blockIdx.x * 256 + tid; r < n; r += (int64_t)gridDim.x * 256) {
-    double sv = w[r];
-    for (int j = 0; j < cnt; ++j) sv = fma(-hs[j], V[(int64_t)j * ldv + r], sv);
+    // four independent chains: four vectors' loads in flight at a time
+    double s0 = w[r], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const double *vr = V + r;
+    int j = 0;
+    for (; j + 4 <= cnt; j += 4) {
+      s0 = fma(-hs[j], vr[(int64_t)j * ldv], s0);
+      s1 = fma(-hs[j + 1], vr[(int64_t)(j + 1) * ldv], s1);
+      s2 = fma(-hs[j + 2], vr[(int64_t)(j + 2) * ldv], s2);
+      s3 = fma(-hs[j + 3], vr[(int64_t)(j + 3) * ldv], s3);
+    }
+    for (; j < cnt; ++j) s0 = fma(-hs[j], vr[(int64_t)j * ldv], s0);
+    const double sv = (s0 + s1) + (s2 + s3);
     w[r] = sv;
     nrm = fma(sv, sv, nrm);
   }
@@ -426,18 +468,25 @@ static Workspace &workspace(nsx_handle *h, int m, int keep, int nev, cudaStream_
   return ws;
 }
 
+// Rows per chunk of k_cg_dot: the vector over RED_CTAS chunks, whole warps, at most CG_CHUNK_MAX.
+constexpr int CG_CHUNK_MAX = 4096;
+static int cg_chunk(int64_t n) {
+  const int64_t per = (n + RED_CTAS - 1) / RED_CTAS;
+  return (int)std::min<int64_t>(CG_CHUNK_MAX, std::max<int64_t>(32, (per + 31) / 32 * 32));
+}
+
 // CGS2 of w against the first cnt basis vectors: h = V^T w, w -= V h, h2 = V^T w, w -= V h2,
 // nrm2 = ||w||^2 (three passes over V, six launches).
 static void cgs2(Workspace &ws, int cnt, double *h, double *h2, double *nrm2, cudaStream_t s) {
   const int64_t n = ws.n;
   const double *V = ws.V;
+  const int chunk = cg_chunk(n);
   count_launch();
-  k_cg_dot<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, ws.w, n, ws.partial);
+  k_cg_dot<<<RED_CTAS, 256, sizeof(double) * chunk, s>>>(V, n, cnt, ws.w, n, chunk, ws.partial);
   count_launch();
   k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h);
-  const size_t smem = sizeof(double) * ((size_t)cnt * (CG_ROWS + 1) + CG_MAXJ + CG_ROWS);
   count_launch();
-  k_cg_subdot<<<RED_CTAS, 256, smem, s>>>(V, n, cnt, h, ws.w, n, ws.partial);
+  k_cg_subdot<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, h, ws.w, n, ws.partial);
   count_launch();
   k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h2);
   count_launch();
@@ -485,8 +534,6 @@ static void ensure_kernel_attributes(int device) {
   if (done.count(device)) return;
   NSX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JACOBI_SMEM_MAX));
   NSX_CUDA(cudaFuncSetAttribute(k_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROTATE_SMEM_MAX));
-  NSX_CUDA(cudaFuncSetAttribute(k_cg_subdot, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(double) * ((size_t)CG_MAXJ * (CG_ROWS + 1) + CG_MAXJ + CG_ROWS))));
   done.insert(device);
 }
 

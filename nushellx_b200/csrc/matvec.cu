@@ -341,22 +341,40 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
 // TC: the FP32 tensor-core form, Zbar tiles in the MMA's swizzled layout (a row of 128 tile
 // columns is 4 contiguous 128-byte lines, so a warp's store is still one full line).
 template <typename T, int NS, bool TC>
+__device__ __forceinline__ void kz_store(T *__restrict__ Zb, const int64_t *zdst, const int *zk, const ZUnit &u, int a,
+                                         int rr, int c, int col, T z) {
+  if constexpr (TC) Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr, c)] = z;
+  else Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
+}
+
+// Rows are taken two at a time (with 16 sources): both rows' loads are in flight together and
+// every weight read from shared memory serves two FMAs.
+template <typename T, int NS, bool TC>
 __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], const int64_t *ysrc, const int64_t *zdst,
                                         const int *zk, int ns, int na, const T *__restrict__ Y, T *__restrict__ Zb) {
   const int c = threadIdx.x;
   if (c >= u.ncols) return;
   const int col = u.c0 + c;
-  for (int rr = 0; rr < u.nr; ++rr) {
+  constexpr int RB = NS <= 16 ? 2 : 1;
+  for (int rr = 0; rr < u.nr; rr += RB) {
+    const bool two = RB == 2 && rr + 1 < u.nr;
     const int64_t roff = (int64_t)(u.row0 + rr) * u.d_bl + col;
-    T y[NS];
+    T y[RB][NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) y[s] = s < ns ? Y[ysrc[s] + roff] : T(0);
+    for (int s = 0; s < NS; ++s) {
+      y[0][s] = s < ns ? Y[ysrc[s] + roff] : T(0);
+      if constexpr (RB == 2) y[1][s] = (s < ns && two) ? Y[ysrc[s] + roff + u.d_bl] : T(0);
+    }
     for (int a = 0; a < na; ++a) {
-      T z = T(0);
+      T z0 = T(0), z1 = T(0);
 #pragma unroll
-      for (int s = 0; s < NS; ++s) z = fma(ws[a][s], y[s], z);
-      if constexpr (TC) Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr, c)] = z;
-      else Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
+      for (int s = 0; s < NS; ++s) {
+        const T wv = ws[a][s];
+        z0 = fma(wv, y[0][s], z0);
+        if constexpr (RB == 2) z1 = fma(wv, y[RB - 1][s], z1);
+      }
+      kz_store<T, NS, TC>(Zb, zdst, zk, u, a, rr, c, col, z0);
+      if (two) kz_store<T, NS, TC>(Zb, zdst, zk, u, a, rr + 1, c, col, z1);
     }
   }
 }
