@@ -55,10 +55,10 @@ REF_ITERS = 300
 # the FP32 variants of the library's H.v (nsx_set_fp32_path); the library picks the fastest
 FP32_VARIANTS = {
     1: "fp32 fused: neutron side formed inside the mixing stage (SIMT FP32, no Y in HBM), proton side on the "
-       "tensor cores (tcgen05.mma kind::tf32, 3xTF32 split, TMEM accumulators, bulk-copy pipeline); like-particle "
-       "part SIMT",
+       "tensor cores (tcgen05.mma kind::tf32, A split into TF32 halves in TMEM, B by bulk copies, 3xTF32, TMEM "
+       "accumulators); like-particle part SIMT",
     2: "fp32 tc: Y in HBM (k_y, mma.sync TF32 3xTF32), mixing into the tensor-core operand layout, proton side on "
-       "the tensor cores (tcgen05.mma kind::tf32, 3xTF32, TMEM accumulators); like-particle part SIMT",
+       "the tensor cores (tcgen05.mma kind::tf32, A in TMEM, 3xTF32, TMEM accumulators); like-particle part SIMT",
     3: "fp32 simt: Y in HBM (k_y, mma.sync TF32 3xTF32), SIMT mixing and proton side (cp.async pipeline); "
        "like-particle part SIMT",
 }

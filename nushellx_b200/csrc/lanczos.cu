@@ -638,7 +638,10 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
 
   std::vector<double> T((size_t)m * m, 0.0), theta, Sm;
   std::vector<double> hcol(m + 2), h2(m + 2);
-  int i0 = 0, i = 0, nconv = 0;
+  int i = 0, nconv = 0;
+  constexpr int CHECK_MIN = 10, CHECK_MAX = 50;   // steps between convergence checks
+  int next_check = 0, last_check_it = -1;
+  double last_dist = 0.0;
   if (resume) {
     // a thick restart from a saved state (the reference's TRL resume, NuCoreX.f90:266-292): the
     // lowest `keep` Ritz vectors of the saved basis, then the saved next vector
@@ -696,7 +699,7 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
     count_launch();
     k_scale<<<grid_for(n), 256, 0, s>>>(ws.w, V(k), ws.h2 + k, n);
     NSX_CUDA(cudaGetLastError());
-    i0 = i = k;
+    i = k;
     iters = std::max(resume->iterations, 0);
     restarts = std::max(resume->restarts, 0) + 1;
   }
@@ -764,7 +767,7 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
       T[(i + 1) + (size_t)m * i] = beta;
       T[i + (size_t)m * (i + 1)] = beta;
     }
-    const bool check = full || exhausted || limit || (((i + 1 - i0) % 10 == 0) && i + 1 >= nev + 2);
+    const bool check = full || exhausted || limit || (iters >= next_check && i + 1 >= nev + 2);
     if (!check) {
       ++i;
       continue;
@@ -776,9 +779,24 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
       for (int r = 0; r < mm; ++r) Tm[r + (size_t)mm * c] = T[r + (size_t)m * c];
     jacobi(ws, mm, Tm, theta, Sm, s);
     nconv = 0;
+    double dist = 0.0;   // log(residual / tol) of the slowest unconverged pair
     for (int j = 0; j < nev && j < mm; ++j) {
       res[j] = std::fabs(beta * Sm[(mm - 1) + (size_t)mm * j]);
       if (res[j] <= tol && nconv == j) ++nconv;
+      if (res[j] > tol) dist = std::max(dist, std::log(res[j] / tol));
+    }
+    // The next check: every check is a Jacobi solve of the projected matrix, so instead of a
+    // fixed interval the residuals' decay since the last check is extrapolated and the next
+    // check placed at 70 % of the steps it predicts to convergence (10 to 50 steps on).
+    {
+      int step = CHECK_MIN;
+      if (last_check_it >= 0 && dist < last_dist && iters > last_check_it) {
+        const double rate = (last_dist - dist) / (double)(iters - last_check_it);
+        step = (int)std::min<double>(CHECK_MAX, std::max<double>(CHECK_MIN, 0.7 * dist / rate));
+      }
+      last_dist = dist;
+      last_check_it = iters;
+      next_check = iters + step;
     }
     if (nconv >= nev || exhausted || limit) {
       // Ritz vectors y_c = V S[:, c], c < nev, into ws.tmp
@@ -831,7 +849,6 @@ void solve(nsx_handle *h, const nsx_params *P, const nsx_state *resume, nsx_stat
     NSX_CUDA(cudaGetLastError());
     std::fill(T.begin(), T.end(), 0.0);
     for (int c = 0; c < keep; ++c) T[c + (size_t)m * c] = theta[c];
-    i0 = keep;
     i = keep;
   }
   tm.flush();
