@@ -176,7 +176,10 @@ int nsx_lcoef(const nsx_handle *h, uint8_t *mask);
 /* Algorithmic flop count of one H.v (partition-sparse, reuse-aware). */
 double nsx_matvec_flops(const nsx_handle *h);
 
-/* y = H x.  x and y are DEVICE pointers of no_state doubles (stream-ordered). */
+/* y = H x.  x and y are DEVICE pointers of no_state doubles (stream-ordered).  The first
+ * product of a handle creates its auxiliary streams and events (the like-particle stage and the
+ * tensor-core classes run beside the main stream, forked from and joined back into it with
+ * events): make it outside a stream capture. */
 int nsx_matvec(nsx_handle *h, const double *x, double *y, int32_t precision, void *stream);
 /* y = H x in FP64 without allocating device memory (no counterpart in the
  * reference).  For callers that cannot have device memory allocated during
@@ -298,7 +301,7 @@ typedef struct nsx_plan_info {
   int64_t tc_tiles[4];        /* k_a_tc tiles with N = 16, 32, 48, 64                         */
   int64_t tc_chunks_max;      /* most 32-row pipeline stages of one k_a_tc tile               */
   int32_t fp32_path;          /* FP32 variant in use (NSX_FP32_*; 0 before the first FP32 H.v) */
-  int32_t pad;
+  int32_t tc_pieces;          /* k_a_tc tiles that are K pieces of a longer slab (atomic sums)  */
 } nsx_plan_info;
 int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out);
 

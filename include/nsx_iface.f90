@@ -77,7 +77,7 @@ module nsx_iface
      integer(c_int32_t) :: y_row_tiles_max, group_sources_max, fused_fp32
      integer(c_int32_t) :: slab_rows_max, slab_splits_max, slab_nl_max
      integer(c_int64_t) :: tc_tiles(4), tc_chunks_max
-     integer(c_int32_t) :: fp32_path, pad
+     integer(c_int32_t) :: fp32_path, tc_pieces
   end type nsx_plan_info
 
   type, bind(C) :: nsx_state

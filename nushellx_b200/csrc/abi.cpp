@@ -424,6 +424,7 @@ int nsx_get_plan_info(const nsx_handle *h, nsx_plan_info *out) {
     for (int c = 0; c < 4; ++c) out->tc_tiles[c] = h->atc_off[c + 1] - h->atc_off[c];
     for (const auto &t : h->atiles_tc) out->tc_chunks_max = std::max<int64_t>(out->tc_chunks_max, (t.kgroups + 3) / 4);
     out->fp32_path = h->fp32_path;
+    for (const auto &t : h->atiles_tc) out->tc_pieces += t.split;
   });
 }
 

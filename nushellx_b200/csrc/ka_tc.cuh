@@ -40,7 +40,10 @@ struct ATileTC {
   int32_t ld;       // d_al (leading dimension of the output block)
   int32_t nl;       // rows of P_l
   int32_t ncols;    // columns of the tile (<= 128)
+  int32_t split;    // 1: one of several K pieces of the slab tile (partial sums added atomically)
+  int32_t pad;
 };
+constexpr int KTC_PIECE_GROUPS = 128;   // 8-row groups per K piece of a long slab (32 stages)
 
 constexpr int KTC_GROUPS = 4;   // 8-row groups per pipeline stage (32 stacked rows)
 
@@ -185,9 +188,15 @@ __global__ void __launch_bounds__(128, KaTcCfg<NPAD>::MIN_CTAS) k_a_tc(const ATi
   if (ok) {
     if (m < t.ncols) {
       float *o = out + t.out + (int64_t)t.ld * m;
+      if (t.split) {
 #pragma unroll
-      for (int i = 0; i < NPAD; ++i)
-        if (i < t.nl) o[i] += acc[i];
+        for (int i = 0; i < NPAD; ++i)
+          if (i < t.nl) atomicAdd(o + i, acc[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < NPAD; ++i)
+          if (i < t.nl) o[i] += acc[i];
+      }
     }
   } else if (tid == 0) {
     atomicOr(err, 1);

@@ -101,11 +101,13 @@ __global__ void __launch_bounds__(256) k_sub(const double *__restrict__ V, int64
     w[i] = s;
   }
 }
-// ---- classical Gram-Schmidt with a second pass (CGS2) in three passes over the basis ----
-// Pass 1 (k_cg_dot):    h  = V^T w                         (V and w read once)
-// Pass 2 (k_cg_subdot): w -= V h, then h2 = V^T w          (V from HBM once: the second read
-//                        of each 128-row chunk of the basis is served from L2)
-// Pass 3 (k_cg_subnrm): w -= V h2, ||w||^2                 (V read once)
+// ---- classical Gram-Schmidt with a second pass (CGS2): four passes over the basis ----
+// k_cg_dot:    h = V^T w                 (V and w read once)
+// k_cg_subnrm: w -= V h                  (V read once, w read and written)
+// k_cg_dot:    h2 = V^T w
+// k_cg_subnrm: w -= V h2, ||w||^2
+// Each pass streams the basis at the HBM roof; a fused subtract-and-dot pass (the second read
+// of each chunk from L2) measured 3x one pass, more than the two passes it replaced.
 // Per-CTA partial sums go to partial[cta][CG_MAXJ] and are added in a fixed order by
 // k_cg_reduce (deterministic).
 constexpr int CG_MAXJ = 128;   // basis vectors per pass (the window is capped below it)
@@ -158,70 +160,6 @@ __global__ void __launch_bounds__(256) k_cg_dot(const double *__restrict__ V, in
   }
 }
 
-// Pass 2 over row chunks of CG_SUB rows: w -= V h for the chunk (two threads per row, each
-// over half of the vectors), the chunk of w kept in shared memory, then warp q forms the
-// chunk's dots with vectors q, q + 8, ...  The second read of the chunk's basis rows follows
-// the first within the CTA, so it is served from L2 (the CTAs' chunks in flight together,
-// 592 x 128 rows x up to 128 vectors, fit in it): V crosses HBM once.
-constexpr int CG_SUB = 128;
-__global__ void __launch_bounds__(256) k_cg_subdot(const double *__restrict__ V, int64_t ldv, int cnt,
-                                                   const double *__restrict__ h, double *__restrict__ w, int64_t n,
-                                                   double *__restrict__ partial) {
-  __shared__ double hs[CG_MAXJ];
-  __shared__ double ws[CG_SUB];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int j = tid; j < cnt; j += 256) hs[j] = h[j];
-  constexpr int JW = CG_MAXJ / 8;
-  double acc[JW];
-#pragma unroll
-  for (int jj = 0; jj < JW; ++jj) acc[jj] = 0.0;
-  const int row = tid >> 1, half = tid & 1;
-  for (int64_t base = (int64_t)blockIdx.x * CG_SUB; base < n; base += (int64_t)gridDim.x * CG_SUB) {
-    const int rows = (int)(n - base < CG_SUB ? n - base : CG_SUB);
-    __syncthreads();   // hs loaded; the previous chunk's ws no longer read
-    {
-      double s0 = 0.0, s1 = 0.0;
-      if (row < rows) {
-        const double *vr = V + base + row;
-        int j = half;
-        for (; j + 2 < cnt; j += 4) {
-          s0 = fma(vr[(int64_t)j * ldv], hs[j], s0);
-          s1 = fma(vr[(int64_t)(j + 2) * ldv], hs[j + 2], s1);
-        }
-        if (j < cnt) s0 = fma(vr[(int64_t)j * ldv], hs[j], s0);
-      }
-      double sv = s0 + s1;
-      sv += __shfl_xor_sync(0xffffffffu, sv, 1);
-      if (half == 0) {
-        const double w1 = row < rows ? w[base + row] - sv : 0.0;
-        ws[row] = w1;
-        if (row < rows) w[base + row] = w1;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int jj = 0; jj < JW; ++jj) {
-      const int j = warp + 8 * jj;
-      if (j < cnt) {
-        const double *vj = V + (int64_t)j * ldv + base;
-        double a = 0.0;
-#pragma unroll
-        for (int q = 0; q < CG_SUB / 32; ++q) {
-          const int r = lane + 32 * q;
-          if (r < rows) a = fma(vj[r], ws[r], a);
-        }
-        acc[jj] += a;
-      }
-    }
-  }
-#pragma unroll
-  for (int jj = 0; jj < JW; ++jj) {
-    const int j = warp + 8 * jj;
-    const double v = warp_sum(acc[jj]);
-    if (lane == 0 && j < cnt) partial[(int64_t)blockIdx.x * CG_MAXJ + j] = v;
-  }
-}
-
 __global__ void __launch_bounds__(256) k_cg_subnrm(const double *__restrict__ V, int64_t ldv, int cnt,
                                                    const double *__restrict__ h, double *__restrict__ w, int64_t n,
                                                    double *__restrict__ partial) {
@@ -232,15 +170,22 @@ __global__ void __launch_bounds__(256) k_cg_subnrm(const double *__restrict__ V,
   __syncthreads();
   double nrm = 0.0;
   for (int64_t r = (int64_t)blockIdx.x * 256 + tid; r < n; r += (int64_t)gridDim.x * 256) {
-    // four independent chains: four vectors' loads in flight at a time
+    // four independent chains
     double s0 = w[r], s1 = 0.0, s2 = 0.0, s3 = 0.0;
     const double *vr = V + r;
     int j = 0;
-    for (; j + 4 <= cnt; j += 4) {
-      s0 = fma(-hs[j], vr[(int64_t)j * ldv], s0);
-      s1 = fma(-hs[j + 1], vr[(int64_t)(j + 1) * ldv], s1);
-      s2 = fma(-hs[j + 2], vr[(int64_t)(j + 2) * ldv], s2);
-      s3 = fma(-hs[j + 3], vr[(int64_t)(j + 3) * ldv], s3);
+    for (; j + 8 <= cnt; j += 8) {   // eight loads issued before their FMAs
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = vr[(int64_t)(j + q) * ldv];
+      s0 = fma(-hs[j], v[0], s0);
+      s1 = fma(-hs[j + 1], v[1], s1);
+      s2 = fma(-hs[j + 2], v[2], s2);
+      s3 = fma(-hs[j + 3], v[3], s3);
+      s0 = fma(-hs[j + 4], v[4], s0);
+      s1 = fma(-hs[j + 5], v[5], s1);
+      s2 = fma(-hs[j + 6], v[6], s2);
+      s3 = fma(-hs[j + 7], v[7], s3);
     }
     for (; j < cnt; ++j) s0 = fma(-hs[j], vr[(int64_t)j * ldv], s0);
     const double sv = (s0 + s1) + (s2 + s3);
@@ -476,21 +421,20 @@ static int cg_chunk(int64_t n) {
 }
 
 // CGS2 of w against the first cnt basis vectors: h = V^T w, w -= V h, h2 = V^T w, w -= V h2,
-// nrm2 = ||w||^2 (three passes over V, six launches).
+// nrm2 = ||w||^2 (four passes over V, seven launches).
 static void cgs2(Workspace &ws, int cnt, double *h, double *h2, double *nrm2, cudaStream_t s) {
   const int64_t n = ws.n;
   const double *V = ws.V;
   const int chunk = cg_chunk(n);
-  count_launch();
-  k_cg_dot<<<RED_CTAS, 256, sizeof(double) * chunk, s>>>(V, n, cnt, ws.w, n, chunk, ws.partial);
-  count_launch();
-  k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h);
-  count_launch();
-  k_cg_subdot<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, h, ws.w, n, ws.partial);
-  count_launch();
-  k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, h2);
-  count_launch();
-  k_cg_subnrm<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, h2, ws.w, n, ws.partial);
+  for (int pass = 0; pass < 2; ++pass) {
+    double *hp = pass == 0 ? h : h2;
+    count_launch();
+    k_cg_dot<<<RED_CTAS, 256, sizeof(double) * chunk, s>>>(V, n, cnt, ws.w, n, chunk, ws.partial);
+    count_launch();
+    k_cg_reduce<<<(cnt + 7) / 8, 256, 0, s>>>(ws.partial, RED_CTAS, cnt, hp);
+    count_launch();
+    k_cg_subnrm<<<RED_CTAS, 256, 0, s>>>(V, n, cnt, hp, ws.w, n, ws.partial);
+  }
   count_launch();
   k_cg_reduce<<<1, 256, 0, s>>>(ws.partial, RED_CTAS, 1, nrm2);
   NSX_CUDA(cudaGetLastError());

@@ -380,34 +380,44 @@ __device__ __forceinline__ void kz_body(const ZUnit &u, const T (*ws)[ZMAXS], co
 }
 
 template <typename T, int NS, bool TC>
-__global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, const ZGroup *__restrict__ groups,
-                                           const ZSrc *__restrict__ srcs, const ZOp *__restrict__ ops,
-                                           const ZOpTC *__restrict__ ops_tc, const T *__restrict__ W,
-                                           const T *__restrict__ Y, T *__restrict__ Zb) {
+__global__ void __launch_bounds__(128) k_z(const ZUnit *__restrict__ units, const int32_t *__restrict__ cta_units,
+                                           const ZGroup *__restrict__ groups, const ZSrc *__restrict__ srcs,
+                                           const ZOp *__restrict__ ops, const ZOpTC *__restrict__ ops_tc,
+                                           const T *__restrict__ W, const T *__restrict__ Y, T *__restrict__ Zb) {
   __shared__ T ws[ZMAXA][ZMAXS];
   __shared__ int64_t ysrc[ZMAXS];
-  __shared__ int64_t zdst[ZMAXA];
-  __shared__ int zk[ZMAXA];
-  const ZUnit u = units[blockIdx.x];
-  const ZGroup G = groups[u.grp];
-  const int na = u.op_end - u.op_begin;
+  __shared__ int64_t zdst[ZMAXA], zbase[ZMAXA];
+  __shared__ int zk[ZMAXA], zkg[ZMAXA];
+  // the CTA's units: consecutive column tiles of one (group, P_r) with the same operators
+  const int ub = cta_units[blockIdx.x], ue = cta_units[blockIdx.x + 1];
+  const ZUnit u0 = units[ub];
+  const ZGroup G = groups[u0.grp];
+  const int na = u0.op_end - u0.op_begin;
   for (int e = threadIdx.x; e < na * ZMAXS; e += blockDim.x) {
     const int a = e / ZMAXS, s = e - a * ZMAXS;
-    ws[a][s] = s < G.ns ? W[G.w_off + ops[u.op_begin + a].wrow * G.ns + s] : T(0);
+    ws[a][s] = s < G.ns ? W[G.w_off + ops[u0.op_begin + a].wrow * G.ns + s] : T(0);
   }
   for (int e = threadIdx.x; e < na; e += blockDim.x) {
     if constexpr (TC) {
-      const ZOpTC o = ops_tc[u.op_begin + e];
-      zdst[e] = o.base + (int64_t)(u.c0 / 128) * o.kgroups * 1024;   // the unit's column tile
+      const ZOpTC o = ops_tc[u0.op_begin + e];
+      zbase[e] = o.base;
+      zkg[e] = o.kgroups;
       zk[e] = o.kofs;
     } else {
-      zdst[e] = ops[u.op_begin + e].z;
+      zdst[e] = ops[u0.op_begin + e].z;
       zk[e] = 0;
     }
   }
   for (int e = threadIdx.x; e < ZMAXS; e += blockDim.x) ysrc[e] = e < G.ns ? srcs[G.s_begin + e].y : 0;
-  __syncthreads();
-  kz_body<T, NS, TC>(u, ws, ysrc, zdst, zk, G.ns, na, Y, Zb);
+  for (int ui = ub; ui < ue; ++ui) {
+    const ZUnit u = ui == ub ? u0 : units[ui];
+    __syncthreads();   // set-up done; the previous unit's destinations no longer read
+    if constexpr (TC) {   // the unit's column tile of each operator's Zbar tiles
+      for (int e = threadIdx.x; e < na; e += blockDim.x) zdst[e] = zbase[e] + (int64_t)(u.c0 / 128) * zkg[e] * 1024;
+      __syncthreads();
+    }
+    kz_body<T, NS, TC>(u, ws, ysrc, zdst, zk, G.ns, na, Y, Zb);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -763,6 +773,7 @@ void upload(nsx_handle *h) {
   d.zgroups = dev_copy_pod(h->zgroups);
   d.zsrcs = dev_copy_pod(h->zsrcs);
   d.zunits = dev_copy_pod(h->zunits);
+  d.zcta = dev_copy_pod(h->zcta);
   d.zops = dev_copy_pod(h->zops);
   d.atiles = dev_copy_pod(h->atiles);
   d.ltiles = dev_copy_pod(h->ltiles);
@@ -878,6 +889,18 @@ void stage_bytes_flops(const nsx_handle *h, int precision, double bytes[NSX_STAG
 // (few tiles with the longest stacked operands) and the other non-empty classes start on
 // the handle's auxiliary streams, forked from and joined back into `s` with events, so that
 // the long tiles overlap the many short ones instead of following them.  Returns the launches.
+// The handle's auxiliary streams and their fork/join events (created on first use).
+static void ensure_aux(nsx_handle *h) {
+  if (h->fork_ev) return;
+  NSX_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+  NSX_CUDA(cudaEventCreateWithFlags(&h->like_fork, cudaEventDisableTiming));
+  NSX_CUDA(cudaEventCreateWithFlags(&h->like_join, cudaEventDisableTiming));
+  for (int i = 0; i < KTC_NCLASS - 1; ++i) {
+    NSX_CUDA(cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
+    NSX_CUDA(cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
+  }
+}
+
 static int launch_ka_tc(nsx_handle *h, const float *Z, float *out, cudaStream_t s) {
   auto &d = h->d;
   int used[KTC_NCLASS], nu = 0;
@@ -885,13 +908,7 @@ static int launch_ka_tc(nsx_handle *h, const float *Z, float *out, cudaStream_t 
     if (h->atc_off[c + 1] > h->atc_off[c]) used[nu++] = c;
   if (nu == 0) return 0;
   if (nu > 1) {
-    if (!h->fork_ev) {
-      NSX_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
-      for (int i = 0; i < KTC_NCLASS - 1; ++i) {
-        NSX_CUDA(cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
-        NSX_CUDA(cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
-      }
-    }
+    ensure_aux(h);
     NSX_CUDA(cudaEventRecord(h->fork_ev, s));
   }
   for (int i = 0; i < nu; ++i) {
@@ -916,14 +933,30 @@ static int launch_ka_tc(nsx_handle *h, const float *Z, float *out, cudaStream_t 
 }
 
 // One product's stages.  path: 0 for FP64; for FP32 the variant (NSX_FP32_FUSED / _TC / _SIMT).
+// fork: the like-particle stage may run on an auxiliary stream (the fixed-scratch entry point
+// keeps everything on the caller's stream and creates nothing).
 template <typename T>
 static void run_stages(nsx_handle *h, int path, const T *x, T *out, const T *rhoB, const T *hA, const T *hB,
-                       const T *w, const T *abar, T *Y, T *Z, cudaStream_t s) {
+                       const T *w, const T *abar, T *Y, T *Z, cudaStream_t s, bool fork = true) {
   auto &d = h->d;
+  // The like-particle stage writes the output block and reads only x: it runs on an auxiliary
+  // stream beside the neutron-side and mixing stages (which never touch the output) and is
+  // joined back before the proton side adds to the output.
+  const bool pn = !h->zunits.empty();
+  bool forked = false;
   if (!h->ltiles.empty()) {
-    StageScope sc(h, 0, s);
-    k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, s>>>(d.ltiles, x, out, hA, hB);
+    cudaStream_t ls = s;
+    if (pn && fork) {
+      ensure_aux(h);
+      NSX_CUDA(cudaEventRecord(h->like_fork, s));
+      NSX_CUDA(cudaStreamWaitEvent(h->aux[0], h->like_fork, 0));
+      ls = h->aux[0];
+      forked = true;
+    }
+    StageScope sc(h, 0, ls);
+    k_like<T><<<(unsigned)h->ltiles.size(), 256, 0, ls>>>(d.ltiles, x, out, hA, hB);
   }
+  if (forked) NSX_CUDA(cudaEventRecord(h->like_join, h->aux[0]));
   constexpr bool F32 = std::is_same<T, float>::value;
   const bool fused = F32 && path == NSX_FP32_FUSED;   // Y formed inside the mixing stage
   const bool tc = F32 && path != NSX_FP32_SIMT;        // proton side on the tensor cores
@@ -942,20 +975,21 @@ static void run_stages(nsx_handle *h, int path, const T *x, T *out, const T *rho
     }
     if (!h->zunits.empty()) {
       StageScope sc(h, 2, s);
-      const unsigned nu = (unsigned)h->zunits.size();
+      const unsigned nu = (unsigned)(h->zcta.size() - 1);
       // sources per group: registers for 16 unless the plan has a larger group
       if (tc) {
         if constexpr (F32) {
-          if (h->max_zns <= 16) k_z<T, 16, true><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
-          else k_z<T, ZMAXS, true><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+          if (h->max_zns <= 16) k_z<T, 16, true><<<nu, 128, 0, s>>>(d.zunits, d.zcta, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+          else k_z<T, ZMAXS, true><<<nu, 128, 0, s>>>(d.zunits, d.zcta, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
         }
       } else if (h->max_zns <= 16) {
-        k_z<T, 16, false><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+        k_z<T, 16, false><<<nu, 128, 0, s>>>(d.zunits, d.zcta, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
       } else {
-        k_z<T, ZMAXS, false><<<nu, 128, 0, s>>>(d.zunits, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
+        k_z<T, ZMAXS, false><<<nu, 128, 0, s>>>(d.zunits, d.zcta, d.zgroups, d.zsrcs, d.zops, d.zops_tc, w, Y, Z);
       }
     }
   }
+  if (forked) NSX_CUDA(cudaStreamWaitEvent(s, h->like_join, 0));   // the output block is written
   if (tc) {
     if constexpr (F32) {
       if (h->atc_off[KTC_NCLASS] > 0) {
@@ -1118,7 +1152,8 @@ void matvec_fp64_with_scratch(nsx_handle *h, const double *x, double *y, double 
   auto &d = h->d;
   h->matvecs++;
   h->last_precision = NSX_FP64;
-  run_stages<double>(h, 0, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s);
+  run_stages<double>(h, 0, x, y, d.rhoB, d.hA, d.hB, d.w, d.abar, scratch, scratch + zbar_scratch_offset(h), s,
+                     false);
 }
 
 // Fails with NSX_E_CUDA if a tensor-core kernel gave up a bounded wait since the last check
@@ -1138,7 +1173,7 @@ void release(nsx_handle *h) {
   auto &d = h->d;
   void *ptrs[] = {d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
                   d.abar_big, d.abar_small, d.zops_tc, d.atiles_tc, d.err,
-                  d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zops, d.atiles, d.ltiles,
+                  d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zcta, d.zops, d.atiles, d.ltiles,
                   d.y64, d.z64, d.y32, d.z32, d.z32r, d.x32, d.o32, d.xin, d.xout};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1150,7 +1185,9 @@ void release(nsx_handle *h) {
     h->join_ev[i] = nullptr;
   }
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
-  h->fork_ev = nullptr;
+  if (h->like_fork) cudaEventDestroy(h->like_fork);
+  if (h->like_join) cudaEventDestroy(h->like_join);
+  h->fork_ev = h->like_fork = h->like_join = nullptr;
   for (auto &e : h->stage_events) {
     cudaEventDestroy(e.second.first);
     cudaEventDestroy(e.second.second);

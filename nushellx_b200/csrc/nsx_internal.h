@@ -138,6 +138,7 @@ struct ZUnit {              // (group, P_r, column tile)
 // KZ_PAD, so that each row of a 128-column tile starts on a 16-byte boundary (asynchronous
 // 16-byte copies into shared memory in k_a, FP32 and FP64); Abar rows likewise (nl -> nlp).
 constexpr int KZ_PAD = 4;
+constexpr int KZ_UNITS_PER_CTA = 8;   // column tiles of one (group, P_r) per k_z CTA
 struct ZOp {
   int64_t z;                // Zbar destination of the operator: element (row rr of P_r, col c) at z + rr*ldz + c
   int32_t wrow;             // weight row within the group
@@ -191,6 +192,7 @@ struct DeviceBuffers {
   ZGroup *zgroups = nullptr;
   ZSrc *zsrcs = nullptr;
   ZUnit *zunits = nullptr;
+  int32_t *zcta = nullptr;   // k_z: first unit of each CTA (consecutive column tiles of one (group, P_r))
   ZOp *zops = nullptr;
   ATile *atiles = nullptr;
   LTile *ltiles = nullptr;
@@ -223,6 +225,7 @@ struct nsx_handle {
   std::vector<nsx::ZGroup> zgroups;
   std::vector<nsx::ZSrc> zsrcs;
   std::vector<nsx::ZUnit> zunits;
+  std::vector<int32_t> zcta;       // k_z CTAs: units [zcta[b], zcta[b+1])
   std::vector<nsx::ZOp> zops;
   std::vector<nsx::ATile> atiles;
   std::vector<double> abar;
@@ -254,6 +257,7 @@ struct nsx_handle {
   // streams and events of the concurrent k_a_tc classes (created on first use)
   cudaStream_t aux[nsx::KTC_NCLASS - 1] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[nsx::KTC_NCLASS - 1] = {};
+  cudaEvent_t like_fork = nullptr, like_join = nullptr;   // the like-particle stage on aux[0]
   // output-block shard: the plan covers the output rows of blocks [own_b0, own_b1), rows
   // [row0, row1); shard_first[r] = first block of rank r (world + 1 entries)
   int shard_rank = 0, shard_world = 1;

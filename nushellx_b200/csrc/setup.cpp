@@ -566,6 +566,16 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
       h->zunits.push_back(u);
     }
   }
+  // k_z CTAs: runs of consecutive units of one (group, P_r) (its column tiles), at most
+  // KZ_UNITS_PER_CTA each, share the CTA's set-up (weights, destinations, sources)
+  h->zcta.clear();
+  for (size_t i = 0; i < h->zunits.size(); ++i) {
+    const ZUnit &u = h->zunits[i];
+    const bool start = h->zcta.empty() || (int)i - h->zcta.back() >= KZ_UNITS_PER_CTA || u.grp != h->zunits[i - 1].grp ||
+                       u.row0 != h->zunits[i - 1].row0 || u.op_begin != h->zunits[i - 1].op_begin;
+    if (start) h->zcta.push_back((int32_t)i);
+  }
+  h->zcta.push_back((int32_t)h->zunits.size());
   // k_a tiles: (slab, KA_TILE_COLS-column tile)
   const int TW = KA_TILE_COLS;
   for (size_t sl = 0; sl < slabs.size(); ++sl) {
@@ -627,17 +637,24 @@ void build_plan(nsx_handle *h, const nsx_problem *p) {
           h->abar_big[e] = b;
           h->abar_small[e] = x - b;
         }
-    for (int t = 0; t * 128 < ob.db; ++t) {
-      ATileTC u;
-      u.zbar = ztc[sl] + (int64_t)t * kg * 1024;
-      u.abar = at;
-      u.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)t * 128 * ob.da;
-      u.kgroups = kg;
-      u.ld = ob.da;
-      u.nl = nl;
-      u.ncols = std::min(128, ob.db - t * 128);
-      tcls[npad / 16 - 1].push_back(u);
-    }
+    // a slab longer than 1.5 pieces is cut into K pieces of KTC_PIECE_GROUPS groups, one CTA
+    // each, so that no single chain of pipeline stages sets the launch's time
+    const int npieces = kg > KTC_PIECE_GROUPS * 3 / 2 ? (kg + KTC_PIECE_GROUPS - 1) / KTC_PIECE_GROUPS : 1;
+    for (int t = 0; t * 128 < ob.db; ++t)
+      for (int pc = 0; pc < npieces; ++pc) {
+        const int g0 = pc * KTC_PIECE_GROUPS, g1 = npieces == 1 ? kg : std::min(kg, g0 + KTC_PIECE_GROUPS);
+        ATileTC u;
+        u.zbar = ztc[sl] + (int64_t)t * kg * 1024 + (int64_t)g0 * 1024;
+        u.abar = at + (int64_t)g0 * 8 * npad;
+        u.out = ob.off + A.poff[A.jidx(ob.J2a)][pl] + (int64_t)t * 128 * ob.da;
+        u.kgroups = g1 - g0;
+        u.ld = ob.da;
+        u.nl = nl;
+        u.ncols = std::min(128, ob.db - t * 128);
+        u.split = npieces > 1 ? 1 : 0;
+        u.pad = 0;
+        tcls[npad / 16 - 1].push_back(u);
+      }
   }
   h->atiles_tc.clear();
   for (int c = 0; c < KTC_NCLASS; ++c) {

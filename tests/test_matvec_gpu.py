@@ -154,7 +154,7 @@ def test_matvec_benchmark_workload_matches_oracle(files_dir):
 # Mid-size cases chosen for the kernel paths they reach (asserted from the plan):
 #  fp 6p+2n J=0+: proton blocks of 3 Y row tiles, FP64 slabs split in up to 17 K pieces,
 #                 proton partitions of up to 49 states (all four tensor-core N classes), the
-#                 fused FP32 neutron/mixing stage, k_a_tc tiles of up to 260 pipeline stages;
+#                 fused FP32 neutron/mixing stage, k_a_tc slabs cut into K pieces (atomic sums);
 #  fp 5p+3n J=1+: mixing groups of 32 sources (FP32 takes k_y + k_z, FP64 the 32-source k_z),
 #                 N classes 16 and 32.
 PATH_CASES = {"fp_6p2n_0": ("FP", 6, 2, 0, 1, 5), "fp_5p3n_2": ("FP", 5, 3, 2, 1, 5)}
@@ -164,7 +164,7 @@ def check_paths(name, info):
     if name == "fp_6p2n_0":
         assert info["y_row_tiles_max"] >= 2 and info["slab_splits_max"] >= 2, info
         assert info["fused_fp32"] == 1 and all(n > 0 for n in info["tc_tiles"]), info
-        assert info["tc_chunks_max"] > 8 and info["slab_nl_max"] > 48, info
+        assert info["tc_chunks_max"] > 8 and info["slab_nl_max"] > 48 and info["tc_pieces"] > 0, info
     else:
         assert info["group_sources_max"] > 16 and info["fused_fp32"] == 0, info
         assert info["tc_tiles"][1] > 0 and info["y_row_tiles_max"] >= 2, info
