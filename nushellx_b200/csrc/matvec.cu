@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
     T *yp = Yt + ws + fc;
     for (int r = tid / W; r < rows; r += 128 / W) {
       T *tp = tile + r * LD + fc;
-      if (fc < wn) yp[(int64_t)r * g.ldy] = *tp;
+      if (fc < wn) __stcs(yp + (int64_t)r * g.ldy, *tp);   // streaming: keep C and rho_B in L2
       *tp = T(0);
     }
     __syncthreads();
@@ -343,8 +343,9 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
 template <typename T, int NS, bool TC>
 __device__ __forceinline__ void kz_store(T *__restrict__ Zb, const int64_t *zdst, const int *zk, const ZUnit &u, int a,
                                          int rr, int c, int col, T z) {
-  if constexpr (TC) Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr, c)] = z;
-  else Zb[zdst[a] + (int64_t)rr * u.ldz + col] = z;
+  // streaming stores: Zbar is read once, by the proton side, long after
+  if constexpr (TC) __stcs(Zb + zdst[a] + umma::a_sw128_index(zk[a] + rr, c), z);
+  else __stcs(Zb + zdst[a] + (int64_t)rr * u.ldz + col, z);
 }
 
 // Rows are taken two at a time (with 16 sources): both rows' loads are in flight together and
