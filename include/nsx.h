@@ -344,7 +344,9 @@ int nsx_set_exchange(nsx_handle *h, nsx_exchange_fn fn, void *user);
  * a Y matrix read by several blocks counts for each of them. */
 int nsx_block_flops(const nsx_handle *h, double *out);
 
-/* Reset the counters; enable (1) or disable (0) per-stage event timing. */
+/* Reset the counters; enable (1) or disable (0) per-stage event timing.  With timing enabled
+ * the stages of a product run one after another (no overlap), so each stage's time is its
+ * own; a product's whole time is then the stages' sum. */
 int nsx_stats_reset(nsx_handle *h, int32_t timing);
 int nsx_get_stats(nsx_handle *h, nsx_stats *out);
 

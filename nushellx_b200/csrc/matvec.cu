@@ -942,12 +942,13 @@ static void run_stages(nsx_handle *h, int path, const T *x, T *out, const T *rho
   auto &d = h->d;
   // The like-particle stage writes the output block and reads only x: it runs on an auxiliary
   // stream beside the neutron-side and mixing stages (which never touch the output) and is
-  // joined back before the proton side adds to the output.
+  // joined back before the proton side adds to the output.  With per-stage timing on, the
+  // stages run one after another, so that each stage's interval is its own.
   const bool pn = !h->zunits.empty();
   bool forked = false;
   if (!h->ltiles.empty()) {
     cudaStream_t ls = s;
-    if (pn && fork) {
+    if (pn && fork && !h->timing) {
       ensure_aux(h);
       NSX_CUDA(cudaEventRecord(h->like_fork, s));
       NSX_CUDA(cudaStreamWaitEvent(h->aux[0], h->like_fork, 0));
