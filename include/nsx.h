@@ -67,6 +67,9 @@ typedef struct nsx_species {
   const int32_t *seg_npr;    /* [nseg] right partition (1-based), >= seg_np      */
   const int64_t *seg_off;    /* [nseg+1] offsets into seg_vals                  */
   const double *seg_vals;    /* matrix(dimptr, dimpt) column-major per segment  */
+  /* occupation of each of the species' nshell shells per partition (the .tri partition record,
+   * [nspart][nshell]); may be null.  With it the result files include NuVec's .xva / .lp. */
+  const int16_t *occ;
 } nsx_species;
 
 typedef struct nsx_problem {

@@ -28,6 +28,7 @@ module nsx_iface
      type(c_ptr)        :: masks
      integer(c_int32_t) :: nseg
      type(c_ptr)        :: seg_J2, seg_np, seg_npr, seg_off, seg_vals
+     type(c_ptr)        :: occ          ! int16 [nspart][nshell] or c_null_ptr
   end type nsx_species
 
   type, bind(C) :: nsx_problem

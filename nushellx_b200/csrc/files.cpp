@@ -49,6 +49,7 @@ constexpr int MAX_CODE = 72;
 
 struct SpeciesStore {
   std::vector<int32_t> njt, par;
+  std::vector<int16_t> occ;   // [nspart][nshell] the species' own shells
   std::vector<uint8_t> keys;
   std::vector<int64_t> val_off;
   std::vector<double> vals;
@@ -91,6 +92,12 @@ void read_species(const nsx_files *f, const char *base, const char *like, int T2
   s.parity = st.par.data();
   s.shell_first = is_proton ? 1 : f->nshells_p + 1;
   s.nshell = is_proton ? f->nshells_p : f->nshells - f->nshells_p;
+  if (s.shell_first - 1 + s.nshell > 32) fail(NSX_E_IO, b + ".tri: more than 32 shells");
+  st.occ.resize((size_t)nspart * s.nshell);
+  for (int p = 0; p < nspart; ++p)
+    for (int o = 0; o < s.nshell; ++o)
+      st.occ[(size_t)p * s.nshell + o] = get<int16_t>(r3.first + 64 * (size_t)p, s.shell_first - 1 + o);
+  s.occ = st.occ.data();
   // .trd
   Records trd(b + ".trd");
   auto d1 = trd.next();

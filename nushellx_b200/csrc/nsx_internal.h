@@ -49,6 +49,7 @@ struct SpeciesPlan {
   int shell_first = 1, nshell = 0;
   std::vector<int> njt;               // [nJ][nspart]
   std::vector<int> par;               // [nspart]
+  std::vector<int16_t> occ;           // [nspart][nshell] shell occupations (empty: not given)
   std::vector<std::vector<int>> poff; // [nJ][nspart+1] partition row offsets inside d(J)
   // densities
   std::vector<uint64_t> keys;         // packed 8-byte keys

@@ -17,6 +17,15 @@
 //   <prefix>.xvc  unformatted sequential, as NuVec writes its eigenvectors (NuVec.f90:182,
 //                 281): record 1: no_state, number of levels (i4); then one record per
 //                 level: energy (r4), vector(1:no_state) (r4)
+//   <prefix>.xva  unformatted sequential, NuVec's averages (NuVec.f90:210-283): one record
+//                 per level: energy (r4), ava(1:no_shells), avb(1:no_shells) (r4: the
+//                 proton and neutron occupation of every shell, weighted by |c|^2), and
+//                 spartpc(no_sparta, no_spartb, min_cJ2a/2:max_cJ2a/2, min_cJ2b/2:max_cJ2b/2)
+//                 (r4, column-major: the percentage of |c|^2 in each partition pair and 2J pair)
+//   <prefix>.lp   formatted: the .lev header, the partitions' shell occupations, and per
+//                 level the average occupations, the parity split and the partition pairs
+//                 holding at least 1 % (NuVec.f90:199-290)
+//                 (.xva and .lp need the partitions' shell occupations, nsx_species.occ)
 //
 // The basis written is the converged Ritz vectors themselves (isave = nev), with
 // matrix = diag(E), alpha = E, betat = 0 and count = 2: NuVec's reconstruction
@@ -82,6 +91,104 @@ double positive_parity_share(const nsx_handle *h, const double *v) {
 }
 }  // namespace
 
+// NuVec's per-level averages: .xva records and the .lp listing (NuVec.f90:199-290).  For each
+// level the squared amplitudes are summed per (proton partition, neutron partition, 2J_a, 2J_b);
+// the shell averages follow from the partition sums and the partitions' shell occupations.
+static void write_xva_lp(const nsx_handle *h, const std::string &base, const double *evals, const double *evecs,
+                         int nev, const char *intfile, int T2) {
+  const SpeciesPlan &A = h->A, &B = h->B;
+  if (A.occ.empty() || B.occ.empty()) return;   // occupations not given: no averages
+  const int64_t n = h->no_state;
+  const int nsa = A.nspart, nsb = B.nspart, nJa = A.nJ, nJb = B.nJ;
+  const int nshells = std::max(A.shell_first - 1 + A.nshell, B.shell_first - 1 + B.nshell);
+  const size_t ncell = (size_t)nsa * nsb * nJa * nJb;
+  RecordWriter xva(base + ".xva");
+  FILE *lp = std::fopen((base + ".lp").c_str(), "w");
+  if (!lp) fail(NSX_E_IO, "cannot write " + base + ".lp");
+  std::fprintf(lp, "  %s\n\n", intfile ? intfile : "");
+  std::fprintf(lp, "  2*J,   2*T %11d %11d\n\n", h->J2, T2);
+  std::fprintf(lp, "  Lowest Energy Levels\n\n");
+  std::fprintf(lp, "\n  Type a = protons   Type b = neutrons\n  A partitions\n");
+  auto partition_line = [&](int p, const SpeciesPlan &S) {
+    std::fprintf(lp, "%8d", -(p + 1));
+    for (int s = 0; s < nshells; ++s) {
+      const int o = s - (S.shell_first - 1);
+      std::fprintf(lp, "%4d", (o >= 0 && o < S.nshell) ? S.occ[(size_t)p * S.nshell + o] : 0);
+    }
+    std::fprintf(lp, "\n");
+  };
+  for (int p = 0; p < nsa; ++p) partition_line(p, A);
+  std::fprintf(lp, "  B partitions\n");
+  for (int p = 0; p < nsb; ++p) partition_line(p, B);
+  std::vector<char> chpar(nev, '?');
+  std::vector<double> cell(ncell), wa(nsa), wb(nsb);
+  for (int i = 0; i < nev; ++i) {
+    const double *v = evecs + (size_t)i * n;
+    std::fill(cell.begin(), cell.end(), 0.0);
+    std::fill(wa.begin(), wa.end(), 0.0);
+    std::fill(wb.begin(), wb.end(), 0.0);
+    double tot = 0.0, pos = 0.0, neg = 0.0;
+    for (const Block &b : h->blocks) {
+      const int ja = A.jidx(b.J2a), jb = B.jidx(b.J2b);
+      int64_t k = b.off;
+      for (int pb = 0; pb < nsb; ++pb)
+        for (int kb = 0; kb < B.njt_of(pb, b.J2b); ++kb)
+          for (int pa = 0; pa < nsa; ++pa) {
+            double s = 0.0;
+            for (int ka = 0; ka < A.njt_of(pa, b.J2a); ++ka, ++k) s += v[k] * v[k];
+            cell[(((size_t)jb * nJa + ja) * nsb + pb) * nsa + pa] += s;
+            wa[pa] += s;
+            wb[pb] += s;
+            tot += s;
+            if (A.par[pa] * B.par[pb] >= 0) pos += s;
+            else neg += s;
+          }
+    }
+    std::vector<float> ava(nshells, 0.f), avb(nshells, 0.f);
+    for (int p = 0; p < nsa; ++p)
+      for (int o = 0; o < A.nshell; ++o) ava[A.shell_first - 1 + o] += (float)(A.occ[(size_t)p * A.nshell + o] * wa[p]);
+    for (int p = 0; p < nsb; ++p)
+      for (int o = 0; o < B.nshell; ++o) avb[B.shell_first - 1 + o] += (float)(B.occ[(size_t)p * B.nshell + o] * wb[p]);
+    const double t = tot > 0 ? tot : 1.0;
+    if (pos / t > 0.95) chpar[i] = '+';
+    if (neg / t > 0.95) chpar[i] = '-';
+    // .xva: E, ava, avb (sums of occupation x |c|^2), spartpc in percent
+    xva.put<float>((float)evals[i]);
+    for (float x : ava) xva.put<float>(x);
+    for (float x : avb) xva.put<float>(x);
+    for (size_t c = 0; c < ncell; ++c) xva.put<float>((float)(cell[c] * 100.0 / t));
+    xva.end_record();
+    // .lp
+    std::fprintf(lp, "\n State %11d %14.6f %c\n\n Average A type nucleons\n", i + 1, evals[i], chpar[i]);
+    for (int s = 0; s < nshells; ++s) std::fprintf(lp, "%7.2f%s", ava[s] / t, (s % 11 == 10 || s == nshells - 1) ? "\n" : "");
+    std::fprintf(lp, "\n Average B type nucleons\n");
+    for (int s = 0; s < nshells; ++s) std::fprintf(lp, "%7.2f%s", avb[s] / t, (s % 11 == 10 || s == nshells - 1) ? "\n" : "");
+    std::fprintf(lp, "  Positive and Negative Parity\n  +ve %8.2f%% -ve %8.2f%%\n", pos * 100.0 / t, neg * 100.0 / t);
+    for (int jb = 0; jb < nJb; ++jb)
+      for (int ja = 0; ja < nJa; ++ja) {
+        double amp = 0.0;
+        for (int pb = 0; pb < nsb; ++pb)
+          for (int pa = 0; pa < nsa; ++pa) amp += cell[(((size_t)jb * nJa + ja) * nsb + pb) * nsa + pa];
+        amp *= 100.0 / t;
+        if (amp < 1.0) continue;
+        std::fprintf(lp, "\n  2*JA, 2*JB, amplitude %11d %11d %14.6f\n", A.minJ2 + 2 * ja, B.minJ2 + 2 * jb, amp);
+        for (int pb = 0; pb < nsb; ++pb) {
+          double ab = 0.0;
+          for (int pa = 0; pa < nsa; ++pa) ab += cell[(((size_t)jb * nJa + ja) * nsb + pb) * nsa + pa];
+          ab *= 100.0 / t;
+          if (ab < 1.0) continue;
+          std::fprintf(lp, "  B partition, amplitude %11d %14.6f\n  A partitions, amplitudes\n", pb + 1, ab);
+          for (int pa = 0; pa < nsa; ++pa)
+            std::fprintf(lp, "(%3d,%7.2f)%s", pa + 1, cell[(((size_t)jb * nJa + ja) * nsb + pb) * nsa + pa] * 100.0 / t,
+                         (pa % 6 == 5 || pa == nsa - 1) ? "\n" : "");
+        }
+      }
+  }
+  std::fprintf(lp, "\n");
+  for (int i = 0; i < nev; ++i) std::fprintf(lp, "%10.3f%c%s", evals[i], chpar[i], (i % 5 == 4 || i == nev - 1) ? "\n" : "");
+  std::fclose(lp);
+}
+
 // NuVec's .xvc eigenvector file and the .lev level list for these eigenpairs.
 static void write_lev_xvc(const nsx_handle *h, const std::string &base, const double *evals, const double *evecs,
                           int nev, const char *intfile, int T2) {
@@ -114,6 +221,7 @@ static void write_lev_xvc(const nsx_handle *h, const std::string &base, const do
     }
     std::fclose(f);
   }
+  write_xva_lp(h, base, evals, evecs, nev, intfile, T2);
 }
 
 void write_results(const nsx_handle *h, const char *prefix, const double *evals, const double *evecs, int nev,

@@ -82,6 +82,8 @@ static void load_species(SpeciesPlan &S, const nsx_species &s, const char *name)
   S.nshell = s.nshell;
   S.njt.assign(s.njt, s.njt + (size_t)S.nJ * S.nspart);
   S.par.assign(s.parity, s.parity + S.nspart);
+  if (s.occ) S.occ.assign(s.occ, s.occ + (size_t)S.nspart * std::max(S.nshell, 0));
+  else S.occ.clear();
   for (int v : S.njt)
     if (v < 0) fail(NSX_E_ARG, std::string("species ") + name + ": negative nJT");
   S.poff.assign(S.nJ, std::vector<int>(S.nspart + 1, 0));

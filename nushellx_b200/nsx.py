@@ -30,7 +30,8 @@ class Species(C.Structure):
                 ("nkeys", C.c_int32), ("keys", _p(C.c_uint8)), ("val_off", _p(C.c_int64)),
                 ("vals", _p(C.c_double)), ("words", C.c_int32), ("masks", _p(C.c_uint32)),
                 ("nseg", C.c_int32), ("seg_J2", _p(C.c_int32)), ("seg_np", _p(C.c_int32)),
-                ("seg_npr", _p(C.c_int32)), ("seg_off", _p(C.c_int64)), ("seg_vals", _p(C.c_double))]
+                ("seg_npr", _p(C.c_int32)), ("seg_off", _p(C.c_int64)), ("seg_vals", _p(C.c_double)),
+                ("occ", _p(C.c_int16))]
 
 
 class Problem(C.Structure):
@@ -89,7 +90,7 @@ class PlanInfo(C.Structure):
                 ("y_row_tiles_max", C.c_int32), ("group_sources_max", C.c_int32), ("fused_fp32", C.c_int32),
                 ("slab_rows_max", C.c_int32), ("slab_splits_max", C.c_int32), ("slab_nl_max", C.c_int32),
                 ("tc_tiles", C.c_int64 * 4), ("tc_chunks_max", C.c_int64), ("fp32_path", C.c_int32),
-                ("pad", C.c_int32)]
+                ("tc_pieces", C.c_int32)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "tc_tiles"}
@@ -192,7 +193,8 @@ def _species_struct(keep, S, dens, segs):
         for k in range(njt.shape[0]):
             njt[k, ip] = S.njt(ip, S.minJ2 + 2 * k)
     par = np.array(S.part_parity, dtype=np.int32)
-    arrs = dict(njt=njt.ravel(), par=par, keys=dens["keys"], val_off=dens["val_off"],
+    occ = np.array(S.parts, dtype=np.int16).reshape(len(S.parts), S.norb)   # shell occupations
+    arrs = dict(njt=njt.ravel(), par=par, occ=occ.ravel(), keys=dens["keys"], val_off=dens["val_off"],
                 vals=np.ascontiguousarray(dens["vals"], dtype=np.float64),
                 masks=np.ascontiguousarray(dens["masks"].ravel(), dtype=np.uint32),
                 sJ=segs["J2"], snp=segs["np"], snpr=segs["npr"], soff=segs["off"],
@@ -216,6 +218,7 @@ def _species_struct(keep, S, dens, segs):
     s.seg_npr = _ptr(arrs["snpr"], C.c_int32)
     s.seg_off = _ptr(arrs["soff"], C.c_int64)
     s.seg_vals = _ptr(arrs["svals"], C.c_double)
+    s.occ = _ptr(arrs["occ"], C.c_int16)
     return s
 
 

@@ -122,3 +122,60 @@ def test_fp32_variant_requests_are_checked():
     T.set_fp32_path(NSX_FP32_TC)
     S.close()
     T.close()
+
+
+def _nuvec_averages(P, S, v):
+    """NuVec's per-level sums (src/NuVec/NuVec.f90:210-240) restated in numpy: |c|^2 per
+    (proton partition, neutron partition, 2J_a, 2J_b), and the shell occupations they weight."""
+    A, B = P.A, P.B
+    nJa, nJb = (A.maxJ2 - A.minJ2) // 2 + 1, (B.maxJ2 - B.minJ2) // 2 + 1
+    cell = np.zeros((nJb, nJa, len(B.parts), len(A.parts)))
+    for k, (J2a, J2b, da, db) in enumerate(S.blocks):
+        blk = v[S.offsets[k]:S.offsets[k + 1]].reshape(db, da)     # column-major: row = neutron state
+        ra = np.repeat(np.arange(len(A.parts)), [A.njt(p, J2a) for p in range(len(A.parts))])
+        rb = np.repeat(np.arange(len(B.parts)), [B.njt(p, J2b) for p in range(len(B.parts))])
+        w = blk ** 2
+        np.add.at(cell[(J2b - B.minJ2) // 2, (J2a - A.minJ2) // 2], (rb[:, None], ra[None, :]), w)
+    wa, wb = cell.sum(axis=(0, 1, 2)), cell.sum(axis=(0, 1, 3))
+    occa = np.array(A.parts, dtype=float)
+    occb = np.array(B.parts, dtype=float)
+    norb = P.space.norb
+    ava = np.concatenate([wa @ occa, np.zeros(norb)])
+    avb = np.concatenate([np.zeros(norb), wb @ occb])
+    return ava, avb, cell
+
+
+@pytest.mark.parametrize("name", ["sd_2p2n_2", "fp_4p4n_0"])
+def test_nuvec_averages_xva_and_lp(name, tmp_path):
+    """.xva / .lp for given eigenpairs, without a GPU: each record holds the energy, the shell
+    occupations weighted by |c|^2 and the partition-pair percentages (NuVec.f90:199-290),
+    equal to the numpy restatement; the percentages add up to 100 and the occupations to the
+    nucleon numbers."""
+    import struct
+    from nushellx_b200.nsx import Solver
+    from test_outputs import read_records
+    P = make_problem(name)
+    S = Solver.from_problem(P, device=-1)
+    rng = np.random.default_rng(3)
+    nev = 3
+    vecs = rng.standard_normal((nev, S.dim)) * S.lcoef
+    vecs /= np.linalg.norm(vecs, axis=1)[:, None]
+    ev = np.array([-3.0, -1.5, 0.25])
+    prefix = str(tmp_path / "av")
+    S.write_results(prefix, ev, vecs, 10, "synthetic", 0)
+    recs = read_records(prefix + ".xva")
+    assert len(recs) == nev
+    norb = P.space.norb
+    for i in range(nev):
+        ava, avb, cell = _nuvec_averages(P, S, vecs[i])
+        r = np.frombuffer(recs[i], dtype="<f4")
+        assert len(r) == 1 + 4 * norb + cell.size
+        assert r[0] == np.float32(ev[i])
+        assert np.allclose(r[1:1 + 2 * norb], ava, atol=1e-5) and np.allclose(r[1 + 2 * norb:1 + 4 * norb], avb, atol=1e-5)
+        sp = r[1 + 4 * norb:].reshape(cell.shape)     # Fortran order (pa fastest, then pb, Ja, Jb)
+        assert np.allclose(sp, cell * 100.0, atol=1e-3)
+        assert abs(sp.sum() - 100.0) < 1e-2
+        assert abs(ava.sum() - P.A.n) < 1e-6 and abs(avb.sum() - P.B.n) < 1e-6
+    lp = open(prefix + ".lp").read()
+    assert lp.count(" State ") == nev and "A partitions" in lp and "Positive and Negative Parity" in lp
+    S.close()
