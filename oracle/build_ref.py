@@ -9,8 +9,12 @@ SRC = os.path.join(HERE, "nsx_ref.c")
 LIB = os.path.join(HERE, "libnsxref.so")
 
 
+HEADER = os.path.join(ROOT, "include", "nsx.h")   # the problem structs it reads
+
+
 def build(force=False):
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
+    newest = max(os.path.getmtime(SRC), os.path.getmtime(HEADER))
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
     # x86-64-v3 (AVX2/FMA): portable across the build host and the GPU hosts' CPUs
     cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c11",
