@@ -344,7 +344,7 @@ template <typename T, int NS, bool TC>
 __device__ __forceinline__ void kz_store(T *__restrict__ Zb, const int64_t *zdst, const int *zk, const ZUnit &u, int a,
                                          int rr, int c, int col, T z) {
   // streaming stores: Zbar is read once, by the proton side, long after
-  if constexpr (TC) __stcs(Zb + zdst[a] + umma::a_sw128_index(zk[a] + rr, c), z);
+  if constexpr (TC) __stcs(Zb + zdst[a] + umma::ztile_index(zk[a] + rr, c), z);
   else __stcs(Zb + zdst[a] + (int64_t)rr * u.ldz + col, z);
 }
 
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(128) k_yz(const ZUnit *__restrict__ units, con
           float z = 0.f;
 #pragma unroll
           for (int sidx = 0; sidx < KYZ_NS; ++sidx) z = fmaf(ws[a][sidx], y[sidx][rb], z);
-          Zb[zdst[a] + umma::a_sw128_index(zk[a] + rr0 + rb, c)] = z;
+          Zb[zdst[a] + umma::ztile_index(zk[a] + rr0 + rb, c)] = z;
         }
       }
     }
