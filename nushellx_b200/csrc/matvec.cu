@@ -302,13 +302,17 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
         nbi = j;
         nlst = hi;
       }
-      if constexpr (std::is_same<T, float>::value) {
-        // tensor cores: warp w owns tile rows [64w, 64w + 64) in two halves of 32
-        const float *Cb = x + g.c_base + g.row0 + m * b.ccol;
+      // FP32: pieces of more than 8 outputs or coefficients on the tensor cores; small ones
+      // (padded to m16n8k8 tiles they would waste most of the MMA work) as SIMT FMAs
+      if (std::is_same<T, float>::value && (hi - l0 > 8 || b.nr > 8)) {
+        if constexpr (std::is_same<T, float>::value) {
+          // tensor cores: warp w owns tile rows [64w, 64w + 64) in two halves of 32
+          const float *Cb = x + g.c_base + g.row0 + m * b.ccol;
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          const int wr0 = 64 * (tid >> 5) + 32 * half;
-          if (wr0 < rows) ky_piece_tc_any(Cb, m, rows, wr0, b.nr, rho + b.rho, b.ldr, l0, hi, tile + (b.ycol - ws), LD);
+          for (int half = 0; half < 2; ++half) {
+            const int wr0 = 64 * (tid >> 5) + 32 * half;
+            if (wr0 < rows) ky_piece_tc_any(Cb, m, rows, wr0, b.nr, rho + b.rho, b.ldr, l0, hi, tile + (b.ycol - ws), LD);
+          }
         }
       } else {
         T *t = tile + tid * LD + (b.ycol - ws);
