@@ -268,6 +268,8 @@ __device__ __forceinline__ void ky_piece_tc_any(const float *C, int64_t m, int r
   }
 }
 
+constexpr int KY_SIMT_MAX = 8;    // FP32 k_y: largest piece (outputs, coefficients) taken as SIMT FMAs
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, const YBlk *__restrict__ blks,
                                            const T *__restrict__ x, const T *__restrict__ rho, T *__restrict__ Y) {
@@ -302,9 +304,9 @@ __global__ void __launch_bounds__(128) k_y(const YGroup *__restrict__ groups, co
         nbi = j;
         nlst = hi;
       }
-      // FP32: pieces of more than 8 outputs or coefficients on the tensor cores; small ones
-      // (padded to m16n8k8 tiles they would waste most of the MMA work) as SIMT FMAs
-      if (std::is_same<T, float>::value && (hi - l0 > 8 || b.nr > 8)) {
+      // FP32: pieces of more than KY_SIMT_MAX outputs or coefficients on the tensor cores; small
+      // ones (padded to m16n8k8 tiles they would waste most of the MMA work) as SIMT FMAs
+      if (std::is_same<T, float>::value && (hi - l0 > KY_SIMT_MAX || b.nr > KY_SIMT_MAX)) {
         if constexpr (std::is_same<T, float>::value) {
           // tensor cores: warp w owns tile rows [64w, 64w + 64) in two halves of 32
           const float *Cb = x + g.c_base + g.row0 + m * b.ccol;
