@@ -196,7 +196,7 @@ int nsx_set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const
     if (!h) fail(NSX_E_ARG, "null handle");
     set_interaction(h, op_vals, nop, a_seg_vals, a_nvals, b_seg_vals, b_nvals);
     DeviceGuard dg(h->device);
-    if (h->device >= 0) upload_interaction(h);
+    if (h->device >= 0) upload_interaction(h, a_seg_vals, b_seg_vals);
   });
 }
 

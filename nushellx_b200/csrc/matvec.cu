@@ -743,22 +743,49 @@ static void dev_refill(T *p, const std::vector<double> &v) {
   NSX_CUDA(cudaMemcpy(p, tmp.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
 }
 
-// Copies the interaction-dependent operands (mixing weights, dense like-particle H) into the
-// device buffers the handle already holds, in every precision that has been set up.  The
-// copies are synchronous, so products issued afterwards on any stream see the new values.
-void upload_interaction(nsx_handle *h) {
+// The segments' values scattered into the dense like-particle H (FP64, and FP32 once that form
+// is set up), both triangles: one CTA per segment (NuOrth's layout, matrix(dimptr, dimpt):
+// value[kr + nr * kl] = H[(np, kl), (npr, kr)]).
+__global__ void k_fill_h(const HSeg *__restrict__ segs, const double *__restrict__ vals, double *__restrict__ hA,
+                         double *__restrict__ hB, float *__restrict__ hA32, float *__restrict__ hB32) {
+  const HSeg g = segs[blockIdx.x];
+  double *H = g.species ? hB : hA;
+  float *H32 = g.species ? hB32 : hA32;
+  const int64_t n = (int64_t)g.nl * g.nr;
+  const bool diag = g.ro == g.co;   // a diagonal segment: entry (kl, kr) with kl >= kr sets both
+  for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+    const int kl = (int)(e / g.nr), kr = (int)(e - (int64_t)kl * g.nr);
+    if (diag && kl < kr) continue;   // (the host fill's order: the later, lower-triangle write wins)
+    const double v = vals[g.v + e];
+    const int64_t i1 = g.h + (g.ro + kl) + (int64_t)g.d * (g.co + kr), i2 = g.h + (g.co + kr) + (int64_t)g.d * (g.ro + kl);
+    H[i1] = v;
+    H[i2] = v;
+    if (H32) {
+      H32[i1] = (float)v;
+      H32[i2] = (float)v;
+    }
+  }
+}
+
+// Copies the interaction-dependent operands into the device buffers the handle already holds, in
+// every precision that has been set up: the mixing weights, and the like-particle segments'
+// values, which k_fill_h scatters into the dense H.  The copies and the scatter complete before
+// return, so products issued afterwards on any stream see the new values.
+void upload_interaction(nsx_handle *h, const double *a_seg_vals, const double *b_seg_vals) {
   NSX_CUDA(cudaDeviceSynchronize());  // no product of the old interaction may still read them
   auto &d = h->d;
   dev_refill<double>(d.w, h->weights);
-  dev_refill<double>(d.hA, h->A.hdense);
-  dev_refill<double>(d.hB, h->B.hdense);
-  if (d.w32) {
-    dev_refill<float>(d.w32, h->weights);
-    dev_refill<float>(d.hA32, h->A.hdense);
-    dev_refill<float>(d.hB32, h->B.hdense);
+  if (d.w32) dev_refill<float>(d.w32, h->weights);
+  const int64_t na = h->A.seg_off.empty() ? 0 : h->A.seg_off.back();
+  const int64_t nb = h->B.seg_off.empty() ? 0 : h->B.seg_off.back();
+  if (na) NSX_CUDA(cudaMemcpy(d.segvals, a_seg_vals, sizeof(double) * na, cudaMemcpyHostToDevice));
+  if (nb) NSX_CUDA(cudaMemcpy(d.segvals + na, b_seg_vals, sizeof(double) * nb, cudaMemcpyHostToDevice));
+  const int nseg = (int)(h->A.seg_J2.size() + h->B.seg_J2.size());
+  if (nseg > 0) {
+    k_fill_h<<<nseg, 256>>>(d.hsegs, d.segvals, d.hA, d.hB, d.hA32, d.hB32);
+    h->launches++;
+    NSX_CUDA(cudaGetLastError());
   }
-  // copies from pageable memory may return before their DMA lands; work on non-blocking
-  // streams is not ordered after them
   NSX_CUDA(cudaDeviceSynchronize());
 }
 
@@ -773,6 +800,31 @@ void upload(nsx_handle *h) {
   d.rhoB = dev_copy<double>(h->yrho);
   d.hA = dev_copy<double>(h->A.hdense);
   d.hB = dev_copy<double>(h->B.hdense);
+  {  // the segment table of the like-particle H (for new interactions)
+    std::vector<HSeg> segs;
+    const SpeciesPlan *sp[2] = {&h->A, &h->B};
+    int64_t vbase = 0;
+    for (int sI = 0; sI < 2; ++sI) {
+      const SpeciesPlan &S = *sp[sI];
+      for (size_t g = 0; g < S.seg_J2.size(); ++g) {
+        const int J2 = S.seg_J2[g], j = S.jidx(J2);
+        const int np = S.seg_np[g] - 1, npr = S.seg_npr[g] - 1;
+        HSeg e;
+        e.h = S.hoff[j];
+        e.v = vbase + S.seg_off[g];
+        e.d = (int32_t)S.poff[j][S.nspart];
+        e.ro = S.poff[j][np];
+        e.co = S.poff[j][npr];
+        e.nl = S.njt_of(np, J2);
+        e.nr = S.njt_of(npr, J2);
+        e.species = sI;
+        segs.push_back(e);
+      }
+      vbase += S.seg_off.empty() ? 0 : S.seg_off.back();
+    }
+    d.hsegs = dev_copy_pod(segs);
+    NSX_CUDA(cudaMalloc(&d.segvals, sizeof(double) * std::max<int64_t>(vbase, 1)));
+  }
   d.w = dev_copy<double>(h->weights);
   d.abar = dev_copy<double>(h->abar);
   d.ygroups = dev_copy_pod(h->ygroups);
@@ -814,8 +866,14 @@ void ensure_precision(nsx_handle *h, int precision) {
     if (!d.x32) {   // the data every FP32 variant reads; each variant's own buffers: ensure_fp32_path
       (void)nz;
       d.rhoB32 = dev_copy<float>(h->yrho);
-      d.hA32 = dev_copy<float>(h->A.hdense);
-      d.hB32 = dev_copy<float>(h->B.hdense);
+      // the FP32 dense H from the device's FP64 copy (the host copy is the plan's: a new
+      // interaction updates the device copy only)
+      const int64_t nA = (int64_t)h->A.hdense.size(), nB = (int64_t)h->B.hdense.size();
+      NSX_CUDA(cudaMalloc(&d.hA32, sizeof(float) * std::max<int64_t>(nA, 1)));
+      NSX_CUDA(cudaMalloc(&d.hB32, sizeof(float) * std::max<int64_t>(nB, 1)));
+      if (nA) k_d2f<<<(unsigned)std::min<int64_t>((nA + 255) / 256, 148 * 16), 256>>>(d.hA, d.hA32, nA);
+      if (nB) k_d2f<<<(unsigned)std::min<int64_t>((nB + 255) / 256, 148 * 16), 256>>>(d.hB, d.hB32, nB);
+      NSX_CUDA(cudaGetLastError());
       d.w32 = dev_copy<float>(h->weights);
       NSX_CUDA(cudaMalloc(&d.x32, h->no_state * sizeof(float)));
       NSX_CUDA(cudaMalloc(&d.o32, h->no_state * sizeof(float)));
@@ -1182,7 +1240,7 @@ void release(nsx_handle *h) {
   void *ptrs[] = {d.rhoB, d.hA, d.hB, d.w, d.abar, d.rhoB32, d.hA32, d.hB32, d.w32, d.abar32,
                   d.abar_big, d.abar_small, d.zops_tc, d.atiles_tc, d.err,
                   d.ygroups, d.yblks, d.zgroups, d.zsrcs, d.zunits, d.zcta, d.zops, d.atiles, d.ltiles,
-                  d.y64, d.z64, d.y32, d.z32, d.z32r, d.x32, d.o32, d.xin, d.xout};
+                  d.y64, d.z64, d.y32, d.z32, d.z32r, d.x32, d.o32, d.xin, d.xout, d.hsegs, d.segvals};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceBuffers();

@@ -169,6 +169,15 @@ struct ZOpTC {
 };
 constexpr int KTC_NCLASS = 4;   // N padded to 16, 32, 48, 64 (nl of the proton partition)
 
+// One like-particle segment of the .mat files in the dense per-J matrix it belongs to: value
+// (kl, kr) of the segment is H[(ro + kl), (co + kr)] and its mirror of the d x d matrix at h.
+struct HSeg {
+  int64_t h;        // element offset of the J block in the species' dense H
+  int64_t v;        // offset of the segment's values in the staging buffer
+  int32_t d, ro, co, nl, nr;
+  int32_t species;  // 0: a (protons), 1: b (neutrons)
+};
+
 // like-particle part: out_blk = Ha C + C Hb, 64x64 output tiles.
 struct LTile {
   int64_t c;        // block offset
@@ -202,6 +211,9 @@ struct DeviceBuffers {
   float *z32r = nullptr;                  // Zbar in the row-major layout of the SIMT proton side, FP32
   float *x32 = nullptr, *o32 = nullptr;
   double *xin = nullptr, *xout = nullptr;  // host-API staging
+  // like-particle segments (a new interaction's values are scattered into the dense H on the GPU)
+  HSeg *hsegs = nullptr;                   // all segments of both species
+  double *segvals = nullptr;               // their values (species a, then b)
 };
 
 }  // namespace nsx
@@ -298,7 +310,7 @@ void require_full_product(const nsx_handle *h);
 void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const double *a_seg_vals, int64_t a_nvals,
                      const double *b_seg_vals, int64_t b_nvals);
 void upload(nsx_handle *h);
-void upload_interaction(nsx_handle *h);
+void upload_interaction(nsx_handle *h, const double *a_seg_vals, const double *b_seg_vals);
 cudaStream_t solve_stream(nsx_handle *h);
 void ensure_precision(nsx_handle *h, int precision);
 void set_fp32_path(nsx_handle *h, int path);

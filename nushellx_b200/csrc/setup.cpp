@@ -179,8 +179,12 @@ void set_interaction(nsx_handle *h, const double *op_vals, int32_t nop, const do
   for (auto &kv : h->vop_index) h->vop[kv.first] = v[kv.second];
   std::fill(h->weights.begin(), h->weights.end(), 0.0);
   for (const WTerm &t : h->wterms) h->weights[t.w] += v[t.op] * t.rw;
-  fill_hdense(h->A, a_seg_vals);
-  fill_hdense(h->B, b_seg_vals);
+  // a device handle fills its dense like-particle H from the segment values on the GPU
+  // (upload_interaction); the host copy is the plan's and stays as built
+  if (h->device < 0) {
+    fill_hdense(h->A, a_seg_vals);
+    fill_hdense(h->B, b_seg_vals);
+  }
 }
 
 void build_plan(nsx_handle *h, const nsx_problem *p) {
