@@ -302,7 +302,7 @@ typedef struct nsx_plan_info {
   int32_t slab_splits_max;    /* most K pieces of one FP64 k_a slab tile (atomic partial sums) */
   int32_t slab_nl_max;        /* most rows of a proton partition (an output slab)             */
   int64_t tc_tiles[4];        /* k_a_tc tiles with N = 16, 32, 48, 64                         */
-  int64_t tc_chunks_max;      /* most 32-row pipeline stages of one k_a_tc tile               */
+  int64_t tc_chunks_max;      /* most 32-row groups of stacked rows in one k_a_tc tile (piece) */
   int32_t fp32_path;          /* FP32 variant in use (NSX_FP32_*; 0 before the first FP32 H.v) */
   int32_t tc_pieces;          /* k_a_tc tiles that are K pieces of a longer slab (atomic sums)  */
 } nsx_plan_info;
