@@ -112,3 +112,29 @@ def test_sharded_solve_reaches_the_unsharded_eigenvalues():
     assert calls[0] == calls[1] > 0
     for S in shards:
         S.close()
+
+
+def test_a_failing_exchange_fails_the_product():
+    """The exchange is the shards' only communication: when it reports a failure (an exception
+    in the host function: a rank gone, a collective timed out), the product fails with an error
+    code and the exception is kept for the caller; the handle stays usable."""
+    from nushellx_b200.build import build
+    from nushellx_b200.nsx import Solver, NSX_FP64, NsxError
+    build()
+    P = make_problem("sd_2p2n_2")
+    S = Solver.from_problem(P, shard=(0, 2))
+
+    def broken(y_ptr, n, stream_ptr):
+        raise TimeoutError("peer rank did not answer")
+
+    S.set_exchange(broken)
+    x = np.random.default_rng(0).standard_normal(S.dim)
+    with pytest.raises(NsxError, match="exchange"):
+        S.matvec_host(x, NSX_FP64)
+    assert isinstance(S.exchange_error, TimeoutError)
+    S.set_exchange(None)   # without an exchange the rank's rows are still computed
+    y = np.full(S.dim, np.nan)
+    S.matvec_host(x, NSX_FP64, out=y)
+    rows = S.shard_info()["rows"]
+    assert not np.any(np.isnan(y[rows[0]:rows[1]])) and np.all(np.isnan(y[rows[1]:]))
+    S.close()
